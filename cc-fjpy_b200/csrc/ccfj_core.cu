@@ -1,0 +1,104 @@
+// Host-side plumbing of the C-ABI: errors, allocator, launch counter.
+#include <atomic>
+#include <mutex>
+
+#include "ccfj_core.cuh"
+
+namespace ccfj {
+
+namespace {
+thread_local std::string g_last_error;
+std::atomic<long long> g_launches{0};
+std::mutex g_alloc_mu;
+ccfj_alloc_fn g_alloc = nullptr;
+ccfj_free_fn g_free = nullptr;
+void* g_alloc_user = nullptr;
+}  // namespace
+
+int set_error(int status, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return status;
+}
+
+void clear_error() { g_last_error.clear(); }
+
+void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+void* dev_alloc(size_t bytes, cudaStream_t s) {
+  if (bytes == 0) bytes = 256;
+  ccfj_alloc_fn fn;
+  void* user;
+  {
+    std::lock_guard<std::mutex> lk(g_alloc_mu);
+    fn = g_alloc;
+    user = g_alloc_user;
+  }
+  if (fn) {
+    void* p = fn(bytes, (void*)s, user);
+    if (!p) set_error(CCFJ_ERR_ALLOC, "allocator hook returned NULL for %zu bytes", bytes);
+    return p;
+  }
+  void* p = nullptr;
+  cudaError_t e = cudaMallocAsync(&p, bytes, s);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    set_error(CCFJ_ERR_ALLOC, "cudaMallocAsync(%zu) failed: %s", bytes, cudaGetErrorString(e));
+    return nullptr;
+  }
+  return p;
+}
+
+void dev_free(void* p, cudaStream_t s) {
+  if (!p) return;
+  ccfj_free_fn fn;
+  void* user;
+  {
+    std::lock_guard<std::mutex> lk(g_alloc_mu);
+    fn = g_free;
+    user = g_alloc_user;
+  }
+  if (fn) {
+    fn(p, (void*)s, user);
+    return;
+  }
+  cudaFreeAsync(p, s);
+}
+
+Scratch::~Scratch() {
+  for (int i = n_ - 1; i >= 0; --i) dev_free(ptrs_[i], s_);
+}
+
+void* Scratch::get(size_t bytes) {
+  if (n_ >= 32) {
+    set_error(CCFJ_ERR_ALLOC, "internal: too many scratch buffers");
+    return nullptr;
+  }
+  void* p = dev_alloc((bytes + 255) & ~size_t(255), s_);
+  if (p) ptrs_[n_++] = p;
+  return p;
+}
+
+}  // namespace ccfj
+
+CCFJ_API const char* ccfj_last_error(void) { return ccfj::g_last_error.c_str(); }
+
+CCFJ_API const char* ccfj_version(void) { return "ccfj_b200 0.1.0 (sm_100a)"; }
+
+CCFJ_API long long ccfj_launch_count(void) {
+  return ccfj::g_launches.load(std::memory_order_relaxed);
+}
+
+CCFJ_API int ccfj_set_allocator(ccfj_alloc_fn alloc, ccfj_free_fn free_fn, void* user) {
+  if ((alloc == nullptr) != (free_fn == nullptr))
+    return ccfj::set_error(CCFJ_ERR_INVALID, "ccfj_set_allocator: give both functions or neither");
+  std::lock_guard<std::mutex> lk(ccfj::g_alloc_mu);
+  ccfj::g_alloc = alloc;
+  ccfj::g_free = free_fn;
+  ccfj::g_alloc_user = user;
+  return CCFJ_OK;
+}

@@ -1,0 +1,179 @@
+// ccfj_fj_earthquake_v1: fj_earthquake and MWFJ from time-domain traces.
+//
+// Reference: src/ccfj-gpu.pyx:270-295 (fj_earthquake) and :297-313 (MWFJ).
+// The reference re-sorts, re-FFTs and re-runs the whole transform (special
+// functions included) once per window; here all windows' spectra come from
+// one batched FFT launch and the transform of each window reuses the same
+// station geometry on the device.
+#include <vector>
+
+#include "ccfj_core.cuh"
+#include "fj_fft.cuh"
+#include "fj_frontend.cuh"
+
+namespace ccfj {
+
+// spec row (w, i) <- TaperSpec of window w and trace row perm[i]
+__global__ void taper_spec_kernel(const int* __restrict__ n1, const int* __restrict__ n2,
+                                  const int* __restrict__ delta, const long long* __restrict__ perm,
+                                  int nwin, int ntr, long long u_rows, TaperSpec* __restrict__ dst) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int w = blockIdx.y;
+  if (i >= ntr) return;
+  const long long row = perm ? perm[i] : i;
+  const long long src = (long long)w * u_rows + row;
+  TaperSpec t;
+  t.n1 = n1[src];
+  t.n2 = n2[src];
+  t.delta = delta[src];
+  t.pad = 0;
+  dst[(long long)w * ntr + i] = t;
+}
+
+static int eq_validate(const ccfj_eq_args* a) {
+  CCFJ_REQUIRE(a != nullptr, "ccfj_fj_earthquake_v1: args is NULL");
+  CCFJ_REQUIRE(a->struct_size == (int)sizeof(ccfj_eq_args),
+               "ccfj_fj_earthquake_v1: struct_size %d != %d (header mismatch)", a->struct_size,
+               (int)sizeof(ccfj_eq_args));
+  CCFJ_REQUIRE(a->ntr >= 1 && a->nf >= 1 && a->nc >= 1 && a->npts >= 2,
+               "ccfj_fj_earthquake_v1: ntr=%d nf=%d nc=%d npts=%d", a->ntr, a->nf, a->nc, a->npts);
+  CCFJ_REQUIRE(a->itype == 0 || a->itype == 1, "ccfj_fj_earthquake_v1: itype must be 0 or 1");
+  CCFJ_REQUIRE(a->func == 0 || a->func == 1, "ccfj_fj_earthquake_v1: func must be 0 or 1");
+  CCFJ_REQUIRE(a->precision >= CCFJ_PREC_FP32 && a->precision <= CCFJ_PREC_FP64_PLAIN,
+               "ccfj_fj_earthquake_v1: bad precision %d", a->precision);
+  CCFJ_REQUIRE(a->fstride >= 1, "ccfj_fj_earthquake_v1: fstride must be >= 1");
+  CCFJ_REQUIRE((long long)(a->nf - 1) * a->fstride <= a->npts / 2,
+               "ccfj_fj_earthquake_v1: bin %lld beyond the last rfft bin %d",
+               (long long)(a->nf - 1) * a->fstride, a->npts / 2);
+  CCFJ_REQUIRE(a->u && a->r && a->f && a->c && a->out, "ccfj_fj_earthquake_v1: NULL array");
+  CCFJ_REQUIRE(a->u_ld >= a->npts, "ccfj_fj_earthquake_v1: u_ld %lld < npts %d", a->u_ld, a->npts);
+  CCFJ_REQUIRE(a->u_rows >= a->ntr, "ccfj_fj_earthquake_v1: u_rows %lld < ntr %d", a->u_rows,
+               a->ntr);
+  CCFJ_REQUIRE(a->nwin >= 0, "ccfj_fj_earthquake_v1: nwin must be >= 0");
+  CCFJ_REQUIRE(a->nwin == 0 || (a->win_n1 && a->win_n2 && a->win_delta),
+               "ccfj_fj_earthquake_v1: nwin > 0 needs win_n1/win_n2/win_delta");
+  return CCFJ_OK;
+}
+
+// All pointers device pointers.
+static int eq_device(const ccfj_eq_args& a, cudaStream_t s) {
+  Scratch sc(s);
+  const int nw = a.nwin > 0 ? a.nwin : 1;
+  const long long rows_out = (long long)nw * a.ntr;
+  float2* spec = sc.get_n<float2>((size_t)rows_out * a.nf);
+  if (!spec) return CCFJ_ERR_ALLOC;
+  TaperSpec* taper = nullptr;
+  if (a.nwin > 0) {
+    taper = sc.get_n<TaperSpec>((size_t)rows_out);
+    if (!taper) return CCFJ_ERR_ALLOC;
+    taper_spec_kernel<<<dim3(div_up(a.ntr, 256), a.nwin), 256, 0, s>>>(
+        a.win_n1, a.win_n2, a.win_delta, a.perm, a.nwin, a.ntr, a.u_rows, taper);
+    count_launch();
+    CCFJ_LAUNCH_CHECK("taper_spec_kernel");
+  }
+  FftJob job{};
+  job.u = a.u;
+  job.u_ld = a.u_ld;
+  job.perm = a.perm;
+  job.ntr = a.ntr;
+  job.npts = a.npts;
+  job.nbins = a.nf;
+  job.bin_stride = a.fstride;
+  job.taper = taper;
+  job.out = spec;
+  int st = rfft_bins(job, (int)rows_out, s, sc);
+  if (st != CCFJ_OK) return st;
+
+  // One transform per window over its [ntr][nf] complex spectra: input 0 is
+  // the real part, input 1 the imaginary part (element stride 2).
+  for (int w = 0; w < nw; ++w) {
+    ccfj_fj_args d{};
+    d.struct_size = sizeof(d);
+    d.nr = a.ntr;
+    d.nf = a.nf;
+    d.nc = a.nc;
+    d.itype = a.itype;
+    d.mode = a.func == 0 ? CCFJ_MODE_ABS_J : CCFJ_MODE_ABS_H;
+    d.precision = a.precision;
+    d.normalize = a.normalize;
+    d.device_ptrs = 1;
+    const float* base = reinterpret_cast<const float*>(spec + (size_t)w * a.ntr * a.nf);
+    d.u[0] = base;
+    d.u[1] = base + 1;
+    d.u_ld = 2LL * a.nf;
+    d.u_rows = a.ntr;
+    d.u_es = 2;
+    d.u_ncols = a.nf;
+    d.fstride = 1;
+    d.r = a.r;
+    d.f = a.f;
+    d.c = a.c;
+    d.out = a.out + (size_t)w * a.nc * a.nf;
+    d.tau = a.tau;
+    st = fj_device(d, s);
+    if (st != CCFJ_OK) return st;
+  }
+  return CCFJ_OK;
+}
+
+static int eq_host(const ccfj_eq_args& a, cudaStream_t s) {
+  if (a.perm)
+    for (int i = 0; i < a.ntr; ++i)
+      CCFJ_REQUIRE(a.perm[i] >= 0 && a.perm[i] < a.u_rows,
+                   "ccfj_fj_earthquake_v1: perm[%d]=%lld out of range", i, a.perm[i]);
+  Scratch sc(s);
+  ccfj_eq_args d = a;
+  d.device_ptrs = 1;
+  const int nw = a.nwin > 0 ? a.nwin : 1;
+  const size_t ubytes = sizeof(float) * ((size_t)(a.u_rows - 1) * a.u_ld + a.npts);
+  float* du = static_cast<float*>(sc.get(ubytes));
+  float* dr = sc.get_n<float>(a.ntr);
+  float* df = sc.get_n<float>(a.nf);
+  float* dc = sc.get_n<float>(a.nc);
+  float* dout = sc.get_n<float>((size_t)nw * a.nc * a.nf);
+  if (!du || !dr || !df || !dc || !dout) return CCFJ_ERR_ALLOC;
+  CCFJ_CUDA_TRY(cudaMemcpyAsync(du, a.u, ubytes, cudaMemcpyHostToDevice, s));
+  CCFJ_CUDA_TRY(cudaMemcpyAsync(dr, a.r, sizeof(float) * a.ntr, cudaMemcpyHostToDevice, s));
+  CCFJ_CUDA_TRY(cudaMemcpyAsync(df, a.f, sizeof(float) * a.nf, cudaMemcpyHostToDevice, s));
+  CCFJ_CUDA_TRY(cudaMemcpyAsync(dc, a.c, sizeof(float) * a.nc, cudaMemcpyHostToDevice, s));
+  if (a.perm) {
+    long long* dp = sc.get_n<long long>(a.ntr);
+    if (!dp) return CCFJ_ERR_ALLOC;
+    CCFJ_CUDA_TRY(cudaMemcpyAsync(dp, a.perm, sizeof(long long) * a.ntr, cudaMemcpyHostToDevice, s));
+    d.perm = dp;
+  }
+  if (a.nwin > 0) {
+    const size_t nwb = sizeof(int) * (size_t)a.nwin * a.u_rows;
+    int* w1 = static_cast<int*>(sc.get(nwb));
+    int* w2 = static_cast<int*>(sc.get(nwb));
+    int* wd = static_cast<int*>(sc.get(nwb));
+    if (!w1 || !w2 || !wd) return CCFJ_ERR_ALLOC;
+    CCFJ_CUDA_TRY(cudaMemcpyAsync(w1, a.win_n1, nwb, cudaMemcpyHostToDevice, s));
+    CCFJ_CUDA_TRY(cudaMemcpyAsync(w2, a.win_n2, nwb, cudaMemcpyHostToDevice, s));
+    CCFJ_CUDA_TRY(cudaMemcpyAsync(wd, a.win_delta, nwb, cudaMemcpyHostToDevice, s));
+    d.win_n1 = w1;
+    d.win_n2 = w2;
+    d.win_delta = wd;
+  }
+  d.u = du;
+  d.r = dr;
+  d.f = df;
+  d.c = dc;
+  d.out = dout;
+  int st = eq_device(d, s);
+  if (st != CCFJ_OK) return st;
+  CCFJ_CUDA_TRY(cudaMemcpyAsync(a.out, dout, sizeof(float) * nw * a.nc * a.nf,
+                                cudaMemcpyDeviceToHost, s));
+  CCFJ_CUDA_TRY(cudaStreamSynchronize(s));
+  return CCFJ_OK;
+}
+
+}  // namespace ccfj
+
+CCFJ_API int ccfj_fj_earthquake_v1(const ccfj_eq_args* args, void* stream) {
+  ccfj::clear_error();
+  int st = ccfj::eq_validate(args);
+  if (st != CCFJ_OK) return st;
+  if (args->device_ptrs) return ccfj::eq_device(*args, (cudaStream_t)stream);
+  return ccfj::eq_host(*args, (cudaStream_t)stream);
+}

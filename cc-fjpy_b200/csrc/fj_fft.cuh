@@ -1,0 +1,31 @@
+// Internal interface of the time-domain front end (see fj_fft.cu).
+#pragma once
+
+#include "ccfj_core.cuh"
+
+namespace ccfj {
+
+// One window of the reference's `win`: zero outside [n1, n2), sine ramps of
+// `delta` samples inside (all integers, computed on the host in float64 the
+// way `win` computes them).
+struct TaperSpec {
+  int n1, n2, delta, pad;
+};
+
+struct FftJob {
+  const float* u;          // traces [rows][u_ld], float32
+  long long u_ld;
+  const long long* perm;   // sorted trace i -> row of u (nullable)
+  int ntr;                 // traces per window
+  int npts;                // samples per trace (FFT length)
+  int nbins;               // output bins per row
+  int bin_stride;          // bin k of output kk is kk * bin_stride
+  int log2n;               // filled in by rfft_bins
+  const TaperSpec* taper;  // [nrows_out] or nullptr
+  float2* out;             // [nrows_out][nbins]
+};
+
+// Runs the front end for nrows_out rows (row = w * ntr + i).
+int rfft_bins(const FftJob& job, int nrows_out, cudaStream_t s, Scratch& sc);
+
+}  // namespace ccfj

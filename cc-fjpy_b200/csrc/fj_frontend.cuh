@@ -1,0 +1,25 @@
+// Internal interfaces between the transform and its device front ends.
+#pragma once
+
+#include "ccfj_core.cuh"
+
+namespace ccfj {
+
+// One input spectrum as the kernels read it: column fi of sorted pair i is
+// p[row(i) * ld + fi * cs], row(i) = perm ? perm[i] : i.
+struct InDesc {
+  const float* p;
+  long long ld;
+  long long cs;
+  const long long* perm;
+};
+
+// dst[i][fi] = (Hilbert transform along the full row of length n, element
+// stride es, of row(i))[fi * fstride]; dst is [nr][nf] float.
+int hilbert_rows(const InDesc& in, int n, int es, int nr, int nf, int fstride, float* dst,
+                 cudaStream_t s, Scratch& sc);
+
+// Device-resident transform (all pointers in args are device pointers).
+int fj_device(const ccfj_fj_args& a, cudaStream_t s);
+
+}  // namespace ccfj

@@ -1,0 +1,370 @@
+// Special functions of the F-J transform, in FP32 (fast path) and FP64
+// (comparator path), compiled for both device and host (host copies back the
+// CPU unit tests of the approximations).
+//
+// What the transform needs at every station x = k r:
+//   Z0(x), Z1(x)   with Z = J (Bessel basis) or Y (Hankel imaginary part)
+//   B(x) = int_0^x Z0(t) dt
+// The reference evaluates these with Numerical-Recipes rational forms and
+// Zhang & Jin Struve series (src/FJcpu.cpp:21-228), twice per interval and in
+// loops of up to 60 terms. Here every function is a fixed-degree polynomial
+// on four ranges (coefficients from gen_fj_special.py, fitted to mpmath
+// values), and the oscillating factor of the x >= 8 range comes from ONE
+// sin/cos pair of chi = x - pi/4 shared by J0, J1, Y0, Y1 and both B's.
+//
+// Phase accuracy: x reaches ~1e4 rad, where an FP32 x carries ~5e-4 rad of
+// error. The caller therefore passes the phase in cycles, t = f r / c, as an
+// unevaluated sum t = p_hi + p_lo (double-float, FP32 only) or as a double;
+// the integer part of t is removed exactly before any rounding.
+#pragma once
+
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+#include "fj_special_coeffs.h"
+
+#ifdef __CUDACC__
+#define FJ_HD __host__ __device__ __forceinline__
+#else
+#define FJ_HD inline
+#endif
+
+namespace fjs {
+
+constexpr float kTwoPiF = 6.28318530717958647692f;
+constexpr double kTwoPi = 6.28318530717958647692;
+constexpr double kPi = 3.14159265358979323846;
+constexpr float kSqrt2OverPiF = 0.79788456080286535588f;  // sqrt(2/pi)
+constexpr double kSqrt2OverPi = 0.79788456080286535588;
+constexpr float kTwoOverPiF = 0.63661977236758134308f;
+constexpr double kTwoOverPi = 0.63661977236758134308;
+
+// ------------------------------------------------------------- primitives
+FJ_HD float fmaT(float a, float b, float c) { return fmaf(a, b, c); }
+FJ_HD double fmaT(double a, double b, double c) { return fma(a, b, c); }
+
+FJ_HD int32_t f2i_bits(float v) {
+#ifdef __CUDA_ARCH__
+  return __float_as_int(v);
+#else
+  int32_t i;
+  memcpy(&i, &v, 4);
+  return i;
+#endif
+}
+FJ_HD float i2f_bits(int32_t i) {
+#ifdef __CUDA_ARCH__
+  return __int_as_float(i);
+#else
+  float v;
+  memcpy(&v, &i, 4);
+  return v;
+#endif
+}
+FJ_HD float rcp_fast(float x) {
+#ifdef __CUDA_ARCH__
+  return __fdividef(1.0f, x);
+#else
+  return 1.0f / x;
+#endif
+}
+FJ_HD float rsqrt_fast(float x) {
+#ifdef __CUDA_ARCH__
+  return rsqrtf(x);
+#else
+  return 1.0f / sqrtf(x);
+#endif
+}
+FJ_HD float log_fast(float x) {
+#ifdef __CUDA_ARCH__
+  return __logf(x);
+#else
+  return logf(x);
+#endif
+}
+
+// Horner evaluation of a fixed coefficient list (lowest degree first).
+template <typename T, int N>
+FJ_HD T horner(const T (&c)[N], T v) {
+  T acc = c[N - 1];
+#pragma unroll
+  for (int i = N - 2; i >= 0; --i) acc = fmaT(acc, v, c[i]);
+  return acc;
+}
+
+// Values at one station for one basis: Z0, Z1 and B = int_0^x Z0.
+template <typename T>
+struct ZB {
+  T z0, z1, b;
+};
+
+// ------------------------------------------------ phase reduction (FP32)
+// Input: the phase of x in cycles, t = p_hi + p_lo (|p_lo| <= ulp(p_hi)).
+// Output: sin and cos of chi = x - pi/4 = 2 pi (t - 1/8).
+//
+// t - 1/8 in quarter turns is 4 t - 1/2. The nearest integer n of p_hi is
+// removed first (p_hi - n is exact), the quarter-turn count q is removed next
+// (a - q exact), and only the remainder v in [-1/2, 1/2] quarter turn is
+// rounded; sin/cos of (pi/2) v are polynomials; q mod 4 rotates them.
+FJ_HD void sincos_chi_f32(float p_hi, float p_lo, float& s_chi, float& c_chi) {
+  // Rounding to an integer by adding and subtracting 1.5 * 2^23 (valid for
+  // |v| < 2^22) keeps the work on the FMA pipe.
+  const float kMagic = 12582912.0f;
+  const float n = (p_hi + kMagic) - kMagic;     // nearest integer of p_hi
+  const float a = fmaT(4.0f, p_hi - n, -0.5f);  // exact
+  const float qm = a + kMagic;                  // rounds a to an integer
+  const int32_t q = f2i_bits(qm);               // low bits hold that integer
+  const float qf = qm - kMagic;
+  const float v = fmaT(4.0f, p_lo, a - qf);
+  const float v2 = v * v;
+  constexpr float cs[] = FJC_F32_SIN;
+  constexpr float cc[] = FJC_F32_COS;
+  const float s = v * horner(cs, v2);
+  const float c = horner(cc, v2);
+  const bool odd = (q & 1) != 0;
+  float ss = odd ? c : s;
+  float cc2 = odd ? s : c;
+  // sin flips for q = 2, 3; cos flips for q = 1, 2
+  ss = i2f_bits(f2i_bits(ss) ^ ((q & 2) << 30));
+  cc2 = i2f_bits(f2i_bits(cc2) ^ (((q + 1) & 2) << 30));
+  s_chi = ss;
+  c_chi = cc2;
+}
+
+// FP64 twin: t in one double (|t| < 2^40 keeps >= 12 bits of fraction).
+FJ_HD void sincos_chi_f64(double t, double& s_chi, double& c_chi) {
+  const double n = rint(t);
+  const double a = 4.0 * (t - n) - 0.5;  // exact up to the rounding of t
+  const double qf = rint(a);
+  const int q = (int)qf;
+  const double v = a - qf;
+  const double v2 = v * v;
+  constexpr double cs[] = FJC_F64_SIN;
+  constexpr double cc[] = FJC_F64_COS;
+  const double s = v * horner(cs, v2);
+  const double c = horner(cc, v2);
+  const bool odd = (q & 1) != 0;
+  double ss = odd ? c : s;
+  double cc2 = odd ? s : c;
+  if (q & 2) ss = -ss;
+  if ((q + 1) & 2) cc2 = -cc2;
+  s_chi = ss;
+  c_chi = cc2;
+}
+
+// ------------------------------------------ station evaluation, FP32
+// x: the argument (FP32, for the smooth parts and the range choice);
+// p_hi + p_lo: x / (2 pi) in cycles (double-float, for the phase).
+// WANT_J / WANT_Y select the basis; WANT_B adds B (itype 1 needs it).
+template <bool WANT_J, bool WANT_Y, bool WANT_B>
+FJ_HD void eval_station_f32(float x, float p_hi, float p_lo, ZB<float>& J, ZB<float>& Y) {
+  if (x >= 8.0f) {
+    float sn, cs;
+    sincos_chi_f32(p_hi, p_lo, sn, cs);
+    const float rs = rsqrt_fast(x);  // one MUFU op gives both 1/sqrt(x) and 1/x
+    const float s = 8.0f * (rs * rs);
+    const float z = s * s;
+    const float M = kSqrt2OverPiF * rs;
+    constexpr float cp0[] = FJC_F32_L_P0;
+    constexpr float cq0[] = FJC_F32_L_Q0;
+    constexpr float cp1[] = FJC_F32_L_P1;
+    constexpr float cq1[] = FJC_F32_L_Q1;
+    const float P0 = horner(cp0, z) * M;
+    const float Q0 = horner(cq0, z) * (s * M);
+    const float P1 = horner(cp1, z) * M;
+    const float Q1 = horner(cq1, z) * (s * M);
+    float rho0 = 0.f, rho1 = 0.f;
+    if (WANT_B) {
+      constexpr float cr0[] = FJC_F32_L_RHO0;
+      constexpr float cr1[] = FJC_F32_L_RHO1;
+      rho0 = horner(cr0, z);
+      rho1 = horner(cr1, z) * s;
+    }
+    if (WANT_J) {
+      J.z0 = fmaT(P0, cs, -Q0 * sn);
+      J.z1 = fmaT(P1, sn, Q1 * cs);
+      if (WANT_B) J.b = fmaT(J.z1, rho0, fmaT(-J.z0, rho1, 1.0f));
+    }
+    if (WANT_Y) {
+      Y.z0 = fmaT(P0, sn, Q0 * cs);
+      Y.z1 = fmaT(Q1, sn, -P1 * cs);
+      if (WANT_B) Y.b = fmaT(Y.z1, rho0, -Y.z0 * rho1);
+    }
+  } else if (x >= 2.0f) {
+    const bool hi = x >= 5.0f;
+    const float u = (x - (hi ? 6.5f : 3.5f)) * (1.0f / 1.5f);
+    if (hi) {
+      if (WANT_J) {
+        constexpr float c0[] = FJC_F32_S2_J0;
+        constexpr float c1[] = FJC_F32_S2_J1;
+        J.z0 = horner(c0, u);
+        J.z1 = horner(c1, u);
+        if (WANT_B) {
+          constexpr float cb[] = FJC_F32_S2_BJ;
+          J.b = horner(cb, u);
+        }
+      }
+      if (WANT_Y) {
+        constexpr float c0[] = FJC_F32_S2_Y0;
+        constexpr float c1[] = FJC_F32_S2_Y1;
+        Y.z0 = horner(c0, u);
+        Y.z1 = horner(c1, u);
+        if (WANT_B) {
+          constexpr float cb[] = FJC_F32_S2_BY;
+          Y.b = horner(cb, u);
+        }
+      }
+    } else {
+      if (WANT_J) {
+        constexpr float c0[] = FJC_F32_S1_J0;
+        constexpr float c1[] = FJC_F32_S1_J1;
+        J.z0 = horner(c0, u);
+        J.z1 = horner(c1, u);
+        if (WANT_B) {
+          constexpr float cb[] = FJC_F32_S1_BJ;
+          J.b = horner(cb, u);
+        }
+      }
+      if (WANT_Y) {
+        constexpr float c0[] = FJC_F32_S1_Y0;
+        constexpr float c1[] = FJC_F32_S1_Y1;
+        Y.z0 = horner(c0, u);
+        Y.z1 = horner(c1, u);
+        if (WANT_B) {
+          constexpr float cb[] = FJC_F32_S1_BY;
+          Y.b = horner(cb, u);
+        }
+      }
+    }
+  } else {
+    const float w = 0.25f * x * x;
+    constexpr float ca[] = FJC_F32_S0_A;
+    constexpr float cb[] = FJC_F32_S0_B;
+    constexpr float cc[] = FJC_F32_S0_C;
+    const float j0 = horner(ca, w);
+    const float j1 = x * horner(cb, w);
+    const float bj = WANT_B ? x * horner(cc, w) : 0.f;
+    if (WANT_J) {
+      J.z0 = j0;
+      J.z1 = j1;
+      if (WANT_B) J.b = bj;
+    }
+    if (WANT_Y) {
+      constexpr float cd[] = FJC_F32_S0_D;
+      constexpr float ce[] = FJC_F32_S0_E;
+      constexpr float cf[] = FJC_F32_S0_F;
+      const float L = kTwoOverPiF * log_fast(0.5f * x);
+      Y.z0 = fmaT(L, j0, horner(cd, w));
+      Y.z1 = fmaT(L, j1, fmaT(x, horner(ce, w), -kTwoOverPiF * rcp_fast(x)));
+      if (WANT_B) Y.b = fmaT(L, bj, x * horner(cf, w));
+    }
+  }
+}
+
+// ------------------------------------------ station evaluation, FP64
+template <bool WANT_J, bool WANT_Y, bool WANT_B>
+FJ_HD void eval_station_f64(double x, double t, ZB<double>& J, ZB<double>& Y) {
+  if (x >= 8.0) {
+    double sn, cs;
+    sincos_chi_f64(t, sn, cs);
+    const double s = 8.0 / x;
+    const double z = s * s;
+    const double M = kSqrt2OverPi / sqrt(x);
+    constexpr double cp0[] = FJC_F64_L_P0;
+    constexpr double cq0[] = FJC_F64_L_Q0;
+    constexpr double cp1[] = FJC_F64_L_P1;
+    constexpr double cq1[] = FJC_F64_L_Q1;
+    const double P0 = horner(cp0, z) * M;
+    const double Q0 = horner(cq0, z) * (s * M);
+    const double P1 = horner(cp1, z) * M;
+    const double Q1 = horner(cq1, z) * (s * M);
+    double rho0 = 0, rho1 = 0;
+    if (WANT_B) {
+      constexpr double cr0[] = FJC_F64_L_RHO0;
+      constexpr double cr1[] = FJC_F64_L_RHO1;
+      rho0 = horner(cr0, z);
+      rho1 = horner(cr1, z) * s;
+    }
+    if (WANT_J) {
+      J.z0 = P0 * cs - Q0 * sn;
+      J.z1 = P1 * sn + Q1 * cs;
+      if (WANT_B) J.b = 1.0 + J.z1 * rho0 - J.z0 * rho1;
+    }
+    if (WANT_Y) {
+      Y.z0 = P0 * sn + Q0 * cs;
+      Y.z1 = Q1 * sn - P1 * cs;
+      if (WANT_B) Y.b = Y.z1 * rho0 - Y.z0 * rho1;
+    }
+  } else if (x >= 2.0) {
+    const bool hi = x >= 5.0;
+    const double u = (x - (hi ? 6.5 : 3.5)) / 1.5;
+    if (hi) {
+      if (WANT_J) {
+        constexpr double c0[] = FJC_F64_S2_J0;
+        constexpr double c1[] = FJC_F64_S2_J1;
+        J.z0 = horner(c0, u);
+        J.z1 = horner(c1, u);
+        if (WANT_B) {
+          constexpr double cb[] = FJC_F64_S2_BJ;
+          J.b = horner(cb, u);
+        }
+      }
+      if (WANT_Y) {
+        constexpr double c0[] = FJC_F64_S2_Y0;
+        constexpr double c1[] = FJC_F64_S2_Y1;
+        Y.z0 = horner(c0, u);
+        Y.z1 = horner(c1, u);
+        if (WANT_B) {
+          constexpr double cb[] = FJC_F64_S2_BY;
+          Y.b = horner(cb, u);
+        }
+      }
+    } else {
+      if (WANT_J) {
+        constexpr double c0[] = FJC_F64_S1_J0;
+        constexpr double c1[] = FJC_F64_S1_J1;
+        J.z0 = horner(c0, u);
+        J.z1 = horner(c1, u);
+        if (WANT_B) {
+          constexpr double cb[] = FJC_F64_S1_BJ;
+          J.b = horner(cb, u);
+        }
+      }
+      if (WANT_Y) {
+        constexpr double c0[] = FJC_F64_S1_Y0;
+        constexpr double c1[] = FJC_F64_S1_Y1;
+        Y.z0 = horner(c0, u);
+        Y.z1 = horner(c1, u);
+        if (WANT_B) {
+          constexpr double cb[] = FJC_F64_S1_BY;
+          Y.b = horner(cb, u);
+        }
+      }
+    }
+  } else {
+    const double w = 0.25 * x * x;
+    constexpr double ca[] = FJC_F64_S0_A;
+    constexpr double cb[] = FJC_F64_S0_B;
+    constexpr double cc[] = FJC_F64_S0_C;
+    const double j0 = horner(ca, w);
+    const double j1 = x * horner(cb, w);
+    const double bj = WANT_B ? x * horner(cc, w) : 0.0;
+    if (WANT_J) {
+      J.z0 = j0;
+      J.z1 = j1;
+      if (WANT_B) J.b = bj;
+    }
+    if (WANT_Y) {
+      constexpr double cd[] = FJC_F64_S0_D;
+      constexpr double ce[] = FJC_F64_S0_E;
+      constexpr double cf[] = FJC_F64_S0_F;
+      const double L = kTwoOverPi * log(0.5 * x);
+      Y.z0 = L * j0 + horner(cd, w);
+      Y.z1 = L * j1 + x * horner(ce, w) - kTwoOverPi / x;
+      if (WANT_B) Y.b = L * bj + x * horner(cf, w);
+    }
+  }
+}
+
+}  // namespace fjs

@@ -1,0 +1,171 @@
+/*
+ * ccfj_b200 -- C ABI of the B200 (sm_100a) frequency-Bessel (F-J) transform.
+ *
+ * Every entry point takes plain pointers and sizes, returns an int status
+ * (CCFJ_OK = 0) and never exits the process or resets the device; on failure
+ * ccfj_last_error() returns a message for the calling thread.
+ *
+ * Array conventions follow the reference (src/FJcpu.cpp:247-256):
+ *   u_f  float32 [nr, nf]   row ir = station pair ir (pairs sorted by r),
+ *                           element index i + ir*nf
+ *   r    float32 [nr]       pair distances (ascending for the F-J method;
+ *                           as in the reference, unsorted input is integrated
+ *                           interval by interval in the given order)
+ *   f    float32 [nf]       frequencies (Hz)
+ *   c    float32 [nc]       phase velocities (same length unit as r per s)
+ *   out  float32 [nc, nf]   element index i + j*nf
+ */
+#ifndef CCFJ_B200_H
+#define CCFJ_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+#define CCFJ_API extern "C" __attribute__((visibility("default")))
+#else
+#define CCFJ_API __attribute__((visibility("default")))
+#endif
+
+/* ------------------------------------------------------------ status codes */
+#define CCFJ_OK 0
+#define CCFJ_ERR_INVALID 1     /* bad argument (size, pointer, enum)        */
+#define CCFJ_ERR_CUDA 2        /* a CUDA runtime call or launch failed      */
+#define CCFJ_ERR_ALLOC 3       /* device or pinned allocation failed        */
+#define CCFJ_ERR_UNSUPPORTED 4 /* valid request this build cannot serve     */
+#define CCFJ_ERR_TIMEOUT 5     /* a bounded device-side wait ran out        */
+
+/* --------------------------------------------- reference-compatible entry
+ * Drop-in for the reference's GPU library (include/FJgpu.hh:13-15), with the
+ * semantics of its CPU library (src/FJcpu.cpp:401-419):
+ *   FJ / FHr : Bessel basis J   (type 1: integral_J, type 0: trap_J)
+ *   FHi      : Hankel basis Y   (type 1: integral_Y, type 0: trap_Y)
+ * All pointers are HOST memory; the call is synchronous; out is overwritten.
+ * The reference's GPU FJ with type 1 ran integral_c (src/FJgpu.cu:315-358),
+ * a truncated odd-Bessel series that does not match its own CPU FJ; this FJ
+ * follows the CPU definition.
+ * Unlike the reference (which returns 0 and leaves out untouched for any
+ * other type), an invalid type returns CCFJ_ERR_INVALID.
+ */
+CCFJ_API int FJ(float *u_f, float *r, float *f, float *out, float *c, int nc, int nr, int nf,
+                int type);
+CCFJ_API int FHr(float *u_f, float *r, float *f, float *out, float *c, int nc, int nr, int nf,
+                 int type);
+CCFJ_API int FHi(float *u_f, float *r, float *f, float *out, float *c, int nc, int nr, int nf,
+                 int type);
+/* The CPU library's Hankel entry (include/FJcpu.h:20); nThread is accepted
+ * and ignored (all work runs on the current CUDA device). */
+CCFJ_API int FH(float *u_f, float *r, float *f, float *out, float *c, int nc, int nr, int nf,
+                int type, int nThread);
+
+/* ------------------------------------------------------ general transform */
+#define CCFJ_MODE_J 0      /* out = FJ(u0)                                      */
+#define CCFJ_MODE_Y 1      /* out = FH(u0)  (Y basis)                           */
+#define CCFJ_MODE_J_MINUS_Y 2 /* out = FJ(u0) - FH(u1)   (fj_noise func=1)       */
+#define CCFJ_MODE_ABS_J 3  /* out = |FJ(u0) + i FJ(u1)|  (fj_earthquake func=0)  */
+#define CCFJ_MODE_ABS_H 4  /* out = |(FJ(u0)-FH(u1)) + i(FJ(u1)+FH(u0))|  (func=1)*/
+
+#define CCFJ_PREC_FP32 0       /* station-amortised FP32 (fast path)           */
+#define CCFJ_PREC_FP64 1       /* station-amortised FP64                        */
+#define CCFJ_PREC_FP64_PLAIN 2 /* reference loop structure in FP64 (comparator) */
+
+typedef struct ccfj_fj_args {
+  int struct_size;     /* sizeof(ccfj_fj_args)                                 */
+  int nr, nf, nc;      /* pairs, frequencies, velocities                       */
+  int itype;           /* 1: linear-interpolation integral, 0: trapezoid       */
+  int mode;            /* CCFJ_MODE_*                                          */
+  int precision;       /* CCFJ_PREC_*                                          */
+  int normalize;       /* 1: out[:, i] /= max|out[:, i]| (reference semantics) */
+  int device_ptrs;     /* 1: every pointer is device memory, call is async on  */
+                       /*    `stream`; 0: host memory, call is synchronous     */
+  int hilbert;         /* 1 (mode J_MINUS_Y only, u[1] = NULL): u[1] is the    */
+                       /*    Hilbert transform of each full row of u[0] along  */
+                       /*    frequency, as scipy.fftpack.hilbert              */
+  const float *u[2];   /* input spectra; u[1] only for two-input modes         */
+  long long u_ld;      /* elements between rows of u (station pairs)           */
+  long long u_rows;    /* rows present in u (>= nr; >= max(perm)+1)            */
+  int u_es;            /* elements between adjacent columns (1: float32 data;  */
+                       /*    2: one part of interleaved complex64 data)        */
+  int u_ncols;         /* columns per row; column j is u[row*u_ld + j*u_es]    */
+  int fstride;         /* frequency i uses column i*fstride (needs            */
+                       /*    ceil(u_ncols/fstride) == nf, as the reference)    */
+  const long long *perm; /* optional [nr]: row of u for sorted pair i          */
+  const float *r;      /* [nr] distances of the sorted pairs                    */
+  const float *f;      /* [nf]                                                  */
+  const float *c;      /* [nc]                                                  */
+  float *out;          /* [nc, nf]                                              */
+  float tau;           /* Hermite/closed-form switch in k*dr; <= 0: default    */
+} ccfj_fj_args;
+
+CCFJ_API int ccfj_fj_v1(const ccfj_fj_args *args, void *stream);
+
+/* ------------------------------------------ earthquake / multi-window F-J
+ * fj_earthquake (src/ccfj-gpu.pyx:270-295) and MWFJ (:297-313) from
+ * time-domain traces: optional taper window, real FFT on the device, F-J of
+ * the real and imaginary parts, magnitude, per-frequency normalisation.
+ *   func 0: out = |FJ(Re) + i FJ(Im)|
+ *   func 1: out = |(FJ(Re) - FH(Im)) + i (FJ(Im) + FH(Re))|
+ * Windows (nwin > 0) are the reference's `win` per (window w, trace j) given
+ * by its integer sample range [n1, n2) and ramp length delta, arrays
+ * [nwin][u_rows] indexed by the row of u (the caller's trace order). The
+ * transform of every window shares one station geometry.
+ */
+typedef struct ccfj_eq_args {
+  int struct_size;     /* sizeof(ccfj_eq_args)                                 */
+  int ntr, npts;       /* traces (= station pairs) and samples per trace       */
+  int nf, nc;          /* frequencies (bins k*fstride, k < nf), velocities     */
+  int itype, func;     /* as ccfj_fj_args.itype; func 0 or 1 (see above)       */
+  int precision;       /* CCFJ_PREC_*                                          */
+  int normalize;       /* per-frequency max-abs normalisation of every window */
+  int device_ptrs;     /* as ccfj_fj_args.device_ptrs                          */
+  int fstride;         /* FFT bin of frequency k is k*fstride                  */
+  int nwin;            /* 0: no window, out is [nc, nf]; else [nwin, nc, nf]   */
+  const float *u;      /* traces, float32 [u_rows][u_ld], npts used            */
+  long long u_ld;
+  long long u_rows;
+  const long long *perm; /* optional [ntr]: row of u of sorted trace i          */
+  const float *r;      /* [ntr] distances of the sorted traces                  */
+  const float *f;      /* [nf]                                                  */
+  const float *c;      /* [nc]                                                  */
+  const int *win_n1;   /* [nwin][u_rows] when nwin > 0                          */
+  const int *win_n2;
+  const int *win_delta;
+  float *out;
+  float tau;           /* as ccfj_fj_args.tau                                   */
+} ccfj_eq_args;
+
+CCFJ_API int ccfj_fj_earthquake_v1(const ccfj_eq_args *args, void *stream);
+
+/* ------------------------------------------------------------------ misc */
+CCFJ_API const char *ccfj_last_error(void);
+CCFJ_API const char *ccfj_version(void);
+/* Kernel launches issued by this library since load (all threads). */
+CCFJ_API long long ccfj_launch_count(void);
+
+/* Optional timing: after ccfj_profile_enable(1) (which also resets the
+ * record), every transform records a pair of CUDA events on its stream
+ * around its main F-J kernel (up to 512 pairs; no synchronisation is added).
+ * ccfj_last_transform_ms() waits for the last pair and returns its duration
+ * in ms (-1 if none); ccfj_profile_total_ms() waits for all of them and
+ * returns the summed ms, with the number of pairs in *count. */
+CCFJ_API int ccfj_profile_enable(int on);
+CCFJ_API float ccfj_last_transform_ms(void);
+CCFJ_API double ccfj_profile_total_ms(int *count);
+/* FP32 FMA throughput of the current device in TFLOP/s (FMA = 2 flops),
+ * measured with independent FMA chains on `stream`: the roofline peak of the
+ * transform kernels, which are bound by the FP32 pipe. */
+CCFJ_API int ccfj_fp32_peak_probe(void *stream, double *tflops);
+
+/* Replaces the device allocator (NULL, NULL restores the default
+ * stream-ordered cudaMallocAsync/cudaFreeAsync). alloc returns NULL on
+ * failure; both receive the cudaStream_t of the call as void*. */
+typedef void *(*ccfj_alloc_fn)(size_t bytes, void *stream, void *user);
+typedef void (*ccfj_free_fn)(void *ptr, void *stream, void *user);
+CCFJ_API int ccfj_set_allocator(ccfj_alloc_fn alloc, ccfj_free_fn free_fn, void *user);
+
+/* Host-side evaluation of the same special-function code the kernels use
+ * (for unit tests of the approximations on machines without a GPU).
+ * precision: CCFJ_PREC_FP32 or CCFJ_PREC_FP64. For each x[i] >= 0 writes
+ * out[6*i .. 6*i+5] = J0, J1, BJ, Y0, Y1, BY with BZ(x) = int_0^x Z0. */
+CCFJ_API int ccfj_special_host(int precision, long long n, const double *x, double *out);
+
+#endif /* CCFJ_B200_H */

@@ -1,0 +1,165 @@
+"""Parity of the CUDA path (through the public API and the C ABI) with the
+FP64 oracle and with the reference's own outputs (golden fixtures).
+
+Tolerance: the error metric is max over (c, f) of |y - y64| / max_c |y64|
+(the absolute error of the normalised spectrum). The CUDA path must be within
+1e-4 of the FP64 oracle, and within (the reference's own error against the
+oracle) + 1e-4 of the reference's outputs.
+"""
+import ctypes
+import warnings
+
+import numpy as np
+import pytest
+
+import cases
+import fj_oracle as O
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-4
+
+
+@pytest.fixture(scope="module")
+def ccfj():
+    import ccfj as m
+    return m
+
+
+def _quiet(fn, *a, **k):
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        return fn(*a, **k)
+
+
+@pytest.mark.parametrize("name", ["noise_small", "noise_ties", "noise_fstride2", "noise_real64"])
+@pytest.mark.parametrize("itype", [0, 1])
+@pytest.mark.parametrize("func", [0, 1])
+def test_fj_noise(ccfj, golden, name, itype, func):
+    case = cases.noise_case(name)
+    args = (case["uf"], case["r"], case["c"], case["f"])
+    y = _quiet(ccfj.fj_noise, *args, fstride=case["fstride"], itype=itype, func=func)
+    assert y.dtype == np.float32 and y.shape == (len(case["c"]), len(case["f"]))
+    y64 = O._normalize(_quiet(O.fj_noise, *args, fstride=case["fstride"], itype=itype, func=func,
+                              normalize=False))
+    err = O.rel_error(y, y64)
+    assert err <= TOL, err
+    ref = golden["%s_i%d_f%d" % (name, itype, func)]
+    ref_err = O.rel_error(ref, y64)
+    assert O.rel_error(y, ref) <= ref_err + TOL
+
+
+@pytest.mark.parametrize("itype", [0, 1])
+@pytest.mark.parametrize("func", [0, 1])
+def test_fj_earthquake(ccfj, golden, itype, func):
+    case = cases.eq_case("eq_small")
+    args = (case["u"], case["r"], case["c"], case["f"])
+    y = _quiet(ccfj.fj_earthquake, *args, itype=itype, func=func)
+    assert y.dtype == np.float32
+    y64 = O._normalize(O.fj_earthquake(*args, itype=itype, func=func, normalize=False))
+    assert O.rel_error(y, y64) <= TOL
+    ref = golden["eq_small_i%d_f%d" % (itype, func)]
+    assert O.rel_error(y, ref) <= O.rel_error(ref, y64) + TOL
+    # f = 0: k = 0, the reference's column is NaN for the integral form
+    if itype == 1:
+        assert np.isnan(ref[:, 0]).all() and np.isnan(y[:, 0]).all()
+
+
+@pytest.mark.parametrize("func", [0, 1])
+def test_mwfj(ccfj, golden, func):
+    case = cases.mwfj_case("mwfj_small")
+    y = _quiet(ccfj.MWFJ, case["u"], case["r"], case["c"], case["f"], case["Fs"], case["nwin"],
+               case["winl"], case["winr"], taper=case["taper"], func=func)
+    assert y.dtype == np.float64 and y.shape == (case["nwin"], len(case["c"]), len(case["f"]))
+    y64 = np.stack([O._normalize(o) for o in O.MWFJ(
+        case["u"], case["r"], case["c"], case["f"], case["Fs"], case["nwin"], case["winl"],
+        case["winr"], taper=case["taper"], func=func, normalize=False)])
+    ref = golden["mwfj_small_i1_f%d" % func]
+    for w in range(case["nwin"]):
+        assert O.rel_error(y[w], y64[w]) <= TOL
+        assert O.rel_error(y[w], ref[w]) <= O.rel_error(ref[w], y64[w]) + TOL
+
+
+@pytest.mark.parametrize("fname,basis", [("FJ", "J"), ("FHr", "J"), ("FHi", "Y"), ("FH", "Y")])
+@pytest.mark.parametrize("itype", [0, 1])
+def test_reference_c_abi(ccfj, lib, golden, fname, basis, itype):
+    """The reference's own entry points with host pointers (raw, unsorted
+    pairs in the given order, no normalisation)."""
+    case = cases.noise_case("raw_small")
+    U = np.ascontiguousarray(np.real(case["uf"]), dtype=np.float32)
+    r32, f32, c32 = (np.ascontiguousarray(case[k], dtype=np.float32) for k in ("r", "f", "c"))
+    nr, nf, nc = len(r32), len(f32), len(c32)
+    out = np.full(nc * nf, np.nan, dtype=np.float32)
+    fp = ctypes.POINTER(ctypes.c_float)
+    P = lambda a: a.ctypes.data_as(fp)  # noqa: E731
+    extra = (8,) if fname == "FH" else ()
+    st = getattr(lib, fname)(P(U), P(r32), P(f32), P(out), P(c32), nc, nr, nf, itype, *extra)
+    assert st == 0, lib.ccfj_last_error()
+    out = out.reshape(nc, nf)
+    y64 = O.fj_transform(U, r32, f32, c32, itype, basis)
+    assert O.rel_error(out, y64) <= TOL
+    ref = golden["raw_%s_i%d" % ("FJ" if basis == "J" else "FH", itype)]
+    assert O.rel_error(out, ref) <= O.rel_error(ref, y64) + TOL
+
+
+@pytest.mark.parametrize("prec", [1, 2])
+@pytest.mark.parametrize("itype", [0, 1])
+@pytest.mark.parametrize("mode", [0, 1])
+def test_fp64_forms_match_oracle(ccfj, prec, itype, mode):
+    """The FP64 station-amortised form and the FP64 comparator with the
+    reference's loop structure agree with the oracle to ~1e-9."""
+    case = cases.noise_case("noise_small")
+    idx = np.argsort(case["r"])
+    U = np.ascontiguousarray(np.real(case["uf"]), dtype=np.float32)
+    rs = case["r"][idx]
+    y = ccfj._transform([U], rs, case["c"], case["f"], 1, itype, mode, perm=idx, precision=prec)
+    y64 = O.fj_transform(U[idx], rs.astype(np.float32), case["f"].astype(np.float32),
+                         case["c"].astype(np.float32), itype, "JY"[mode])
+    assert O.rel_error(y, y64) <= 1e-6
+
+
+def test_unsorted_pairs_follow_reference_order(ccfj):
+    """fj() does not sort (src/ccfj-gpu.pyx:181-200): reversed intervals are
+    integrated as given, like the reference."""
+    case = cases.noise_case("noise_small")
+    U = np.ascontiguousarray(np.real(case["uf"]), dtype=np.float32)
+    y = ccfj.fj(U, case["r"], case["c"], case["f"], itype=1)
+    y64 = O.fj_transform(U, case["r"].astype(np.float32), case["f"].astype(np.float32),
+                         case["c"].astype(np.float32), 1, "J")
+    assert O.rel_error(y, y64) <= TOL
+
+
+def test_deterministic(ccfj):
+    case = cases.noise_case("noise_small")
+    a = _quiet(ccfj.fj_noise, case["uf"], case["r"], case["c"], case["f"], func=1)
+    b = _quiet(ccfj.fj_noise, case["uf"], case["r"], case["c"], case["f"], func=1)
+    assert np.array_equal(a, b, equal_nan=True)
+
+
+@pytest.mark.parametrize("nr", [1, 2, 3])
+def test_tiny_pair_counts(ccfj, nr):
+    rng = np.random.default_rng(nr)
+    r = rng.uniform(1e3, 2e4, nr)
+    f = np.linspace(0.05, 0.5, 12)
+    c = np.linspace(1000, 4000, 9)
+    uf = cases.noise_spectra(rng, r, f)
+    for itype in (0, 1):
+        y = _quiet(ccfj.fj_noise, uf, r, c, f, itype=itype, normalize=False) \
+            if False else _quiet(ccfj._transform, [np.real(uf)], np.sort(r), c, f, 1, itype, 0,
+                                 perm=np.argsort(r))
+        y64 = O.fj_transform(np.real(uf)[np.argsort(r)], np.sort(r).astype(np.float32),
+                             f.astype(np.float32), c.astype(np.float32), itype, "J")
+        if nr == 1:
+            assert np.all(y == 0)
+        else:
+            assert O.rel_error(y, y64) <= TOL
+
+
+def test_invalid_func_and_shape(ccfj, capsys):
+    case = cases.noise_case("noise_small")
+    assert ccfj.fj_noise(case["uf"], case["r"], case["c"], case["f"], func=3) == 0
+    assert "set func as 0" in capsys.readouterr().out
+    with pytest.raises(ValueError, match="cannot reshape"):
+        ccfj.fj_noise(case["uf"][:, :-1], case["r"], case["c"], case["f"])
+    eq = cases.eq_case("eq_small")
+    with pytest.raises(ValueError, match="cannot reshape"):
+        ccfj.fj_earthquake(eq["u"], eq["r"], eq["c"], eq["f"], fstride=2)

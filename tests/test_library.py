@@ -1,0 +1,83 @@
+"""The C-ABI library: builds, loads, exports every declared symbol, and
+rejects bad arguments before touching the device (no GPU needed)."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import REPO
+
+
+def declared_symbols():
+    text = open(os.path.join(REPO, "include", "ccfj_b200.h")).read()
+    return re.findall(r"CCFJ_API\s+[\w\s\*]+?\b(\w+)\s*\(", text)
+
+
+def test_header_declares_entry_points():
+    syms = declared_symbols()
+    for name in ("FJ", "FHr", "FHi", "FH", "ccfj_fj_v1", "ccfj_fj_earthquake_v1",
+                 "ccfj_last_error", "ccfj_set_allocator", "ccfj_special_host"):
+        assert name in syms
+
+
+def test_library_exports_every_declared_symbol(lib):
+    for name in declared_symbols():
+        assert hasattr(lib, name), name
+
+
+def test_version(lib):
+    assert b"sm_100a" in lib.ccfj_version()
+
+
+def _args(**kw):
+    from ccfj import _lib
+    a = _lib.FjArgs()
+    a.struct_size = ctypes.sizeof(_lib.FjArgs)
+    a.nr, a.nf, a.nc = 4, 3, 2
+    a.itype, a.mode, a.precision = 1, 0, 0
+    a.u_ld, a.u_es, a.u_ncols, a.u_rows, a.fstride = 3, 1, 3, 4, 1
+    buf = np.zeros(64, dtype=np.float32)
+    a.u[0] = buf.ctypes.data
+    a.r = a.f = a.c = a.out = buf.ctypes.data
+    for k, v in kw.items():
+        setattr(a, k, v)
+    return a, buf
+
+
+@pytest.mark.parametrize("field,value,needle", [
+    ("struct_size", 8, "struct_size"),
+    ("itype", 2, "itype"),
+    ("mode", 9, "mode"),
+    ("precision", 7, "precision"),
+    ("nr", 0, "nr="),
+    ("fstride", 0, "fstride"),
+    ("u_ncols", 5, "frequencies"),
+    ("u_rows", 2, "u_rows"),
+])
+def test_invalid_arguments_are_rejected(lib, field, value, needle):
+    a, _buf = _args(**{field: value})
+    st = lib.ccfj_fj_v1(ctypes.byref(a), None)
+    assert st == 1  # CCFJ_ERR_INVALID
+    assert needle in lib.ccfj_last_error().decode()
+
+
+def test_two_input_mode_needs_second_input(lib):
+    a, _buf = _args(mode=2)
+    assert lib.ccfj_fj_v1(ctypes.byref(a), None) == 1
+    assert "two inputs" in lib.ccfj_last_error().decode()
+
+
+def test_compat_entry_rejects_bad_type(lib):
+    fp = ctypes.POINTER(ctypes.c_float)
+    b = np.zeros(16, dtype=np.float32)
+    p = b.ctypes.data_as(fp)
+    assert lib.FJ(p, p, p, p, p, 2, 2, 2, 5) == 1
+
+
+def test_allocator_hook_validation(lib):
+    cb = ctypes.CFUNCTYPE(ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p, ctypes.c_void_p)(
+        lambda n, s, u: None)
+    assert lib.ccfj_set_allocator(ctypes.cast(cb, ctypes.c_void_p), None, None) == 1
+    assert lib.ccfj_set_allocator(None, None, None) == 0

@@ -1,0 +1,65 @@
+"""The special-function approximations of the kernels (host-compiled copy of
+the same source) against mpmath: J0, J1, Y0, Y1 and B = int_0^x Z0."""
+import ctypes
+
+import mpmath as mp
+import numpy as np
+import pytest
+
+mp.mp.dps = 30
+
+
+def _mp_values(x):
+    xm = mp.mpf(x)
+    j0, j1, y0, y1 = mp.besselj(0, xm), mp.besselj(1, xm), mp.bessely(0, xm), mp.bessely(1, xm)
+    h0, h1 = mp.struveh(0, xm), mp.struveh(1, xm)
+    bj = xm * j0 + mp.pi * xm / 2 * (j1 * h0 - j0 * h1)
+    by = xm * y0 + mp.pi * xm / 2 * (y1 * h0 - y0 * h1)
+    return [float(v) for v in (j0, j1, bj, y0, y1, by)]
+
+
+XS = np.concatenate([np.linspace(0.02, 12, 240), np.geomspace(12, 2e4, 160),
+                     [1.999999, 2.0, 4.9999, 5.0, 7.99999, 8.0, 8.00001]])
+REF = np.array([_mp_values(x) for x in XS])
+
+
+def _eval(lib, prec):
+    out = np.zeros((len(XS), 6))
+    st = lib.ccfj_special_host(prec, len(XS), XS.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                               out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    assert st == 0
+    return out
+
+
+def _amplitude(x):
+    # the oscillation amplitude sqrt(2/(pi x)) for x > 1, 1 below
+    return np.minimum(1.0, np.sqrt(2 / (np.pi * np.maximum(x, 1e-30))))
+
+
+def test_fp32_functions(lib):
+    got = _eval(lib, 0)
+    amp = _amplitude(XS)
+    for j, name in enumerate(("J0", "J1", "BJ", "Y0", "Y1", "BY")):
+        scale = amp if name[0] != "B" else np.maximum(amp, np.abs(REF[:, j]))
+        if name in ("Y0", "Y1", "BY"):
+            scale = np.maximum(scale, np.abs(REF[:, j]))
+        err = np.abs(got[:, j] - REF[:, j]) / scale
+        assert err.max() < 1.5e-6, (name, err.max(), XS[err.argmax()])
+
+
+def test_fp64_functions(lib):
+    got = _eval(lib, 1)
+    amp = _amplitude(XS)
+    for j, name in enumerate(("J0", "J1", "BJ", "Y0", "Y1", "BY")):
+        scale = np.maximum(amp, np.abs(REF[:, j]))
+        # the host harness forms the phase as x / (2 pi) in double, which is
+        # already off by about x * 1e-16 rad (the kernels form it from f r / c)
+        err = np.abs(got[:, j] - REF[:, j]) / scale / (1e-13 + 3e-16 * XS)
+        assert err.max() < 1.0, (name, err.max(), XS[err.argmax()])
+
+
+def test_bad_precision(lib):
+    x = np.ones(1)
+    out = np.zeros(6)
+    assert lib.ccfj_special_host(2, 1, x.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                 out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))) == 1
