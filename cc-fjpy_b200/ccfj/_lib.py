@@ -73,6 +73,8 @@ SIGNATURES = {
     "ccfj_special_host": (ctypes.c_int, [ctypes.c_int, ctypes.c_longlong,
                                          ctypes.POINTER(ctypes.c_double),
                                          ctypes.POINTER(ctypes.c_double)]),
+    "ccfj_special_device": (ctypes.c_int, [ctypes.c_int, ctypes.c_longlong, ctypes.c_void_p,
+                                           ctypes.c_void_p, ctypes.c_void_p]),
 }
 
 _LIB = None

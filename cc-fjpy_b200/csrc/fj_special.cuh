@@ -99,40 +99,12 @@ struct ZB {
   T z0, z1, b;
 };
 
-// ------------------------------------------------ phase reduction (FP32)
-// Input: the phase of x in cycles, t = p_hi + p_lo (|p_lo| <= ulp(p_hi)).
-// Output: sin and cos of chi = x - pi/4 = 2 pi (t - 1/8).
-//
-// t - 1/8 in quarter turns is 4 t - 1/2. The nearest integer n of p_hi is
-// removed first (p_hi - n is exact), the quarter-turn count q is removed next
-// (a - q exact), and only the remainder v in [-1/2, 1/2] quarter turn is
-// rounded; sin/cos of (pi/2) v are polynomials; q mod 4 rotates them.
-FJ_HD void sincos_chi_f32(float p_hi, float p_lo, float& s_chi, float& c_chi) {
-  // Rounding to an integer by adding and subtracting 1.5 * 2^23 (valid for
-  // |v| < 2^22) keeps the work on the FMA pipe.
-  const float kMagic = 12582912.0f;
-  const float n = (p_hi + kMagic) - kMagic;     // nearest integer of p_hi
-  const float a = fmaT(4.0f, p_hi - n, -0.5f);  // exact
-  const float qm = a + kMagic;                  // rounds a to an integer
-  const int32_t q = f2i_bits(qm);               // low bits hold that integer
-  const float qf = qm - kMagic;
-  const float v = fmaT(4.0f, p_lo, a - qf);
-  const float v2 = v * v;
-  constexpr float cs[] = FJC_F32_SIN;
-  constexpr float cc[] = FJC_F32_COS;
-  const float s = v * horner(cs, v2);
-  const float c = horner(cc, v2);
-  const bool odd = (q & 1) != 0;
-  float ss = odd ? c : s;
-  float cc2 = odd ? s : c;
-  // sin flips for q = 2, 3; cos flips for q = 1, 2
-  ss = i2f_bits(f2i_bits(ss) ^ ((q & 2) << 30));
-  cc2 = i2f_bits(f2i_bits(cc2) ^ (((q + 1) & 2) << 30));
-  s_chi = ss;
-  c_chi = cc2;
-}
-
-// FP64 twin: t in one double (|t| < 2^40 keeps >= 12 bits of fraction).
+// ------------------------------------------------ phase reduction (FP64)
+// t = x / (2 pi) in cycles as one double (|t| < 2^40 keeps >= 12 bits of
+// fraction). Output: sin and cos of chi = x - pi/4 = 2 pi (t - 1/8). The
+// integer part n of t is removed first (t - n is exact), the quarter-turn
+// count q next (a - q exact); sin/cos of (pi/2) v, |v| <= 1/2, are
+// polynomials and q mod 4 rotates them.
 FJ_HD void sincos_chi_f64(double t, double& s_chi, double& c_chi) {
   const double n = rint(t);
   const double a = 4.0 * (t - n) - 0.5;  // exact up to the rounding of t
@@ -153,43 +125,73 @@ FJ_HD void sincos_chi_f64(double t, double& s_chi, double& c_chi) {
   c_chi = cc2;
 }
 
+// ------------------------------------------------ phase reduction, fast
+// chi / (2 pi) = t - 1/8 reduced to [-5/8, 1/2] cycles: the integer part of
+// p_hi is removed exactly (p_hi - n is exact), p_lo and the 1/8 shift are
+// added after, so the only rounding is that of the final sum (< 3e-8 cycle).
+FJ_HD float chi_cycles_f32(float p_hi, float p_lo) {
+  const float kMagic = 12582912.0f;  // 1.5 * 2^23: x + M - M rounds |x| < 2^22
+  const float n = (p_hi + kMagic) - kMagic;
+  return (p_hi - n) + (p_lo - 0.125f);
+}
+
+// sin and cos of 2 pi u for |u| <= 5/8. On the device this is the SFU's
+// sine/cosine (two MUFU ops, absolute error about 4e-7 on this range); the
+// host build (used by the CPU tests of the polynomials) uses libm.
+FJ_HD void sincos_cycles_f32(float u, float& s, float& c) {
+#ifdef __CUDA_ARCH__
+  __sincosf(kTwoPiF * u, &s, &c);
+#else
+  const double a = kTwoPi * (double)u;
+  s = (float)sin(a);
+  c = (float)cos(a);
+#endif
+}
+
 // ------------------------------------------ station evaluation, FP32
 // x: the argument (FP32, for the smooth parts and the range choice);
 // p_hi + p_lo: x / (2 pi) in cycles (double-float, for the phase).
-// WANT_J / WANT_Y select the basis; WANT_B adds B (itype 1 needs it).
-template <bool WANT_J, bool WANT_Y, bool WANT_B>
-FJ_HD void eval_station_f32(float x, float p_hi, float p_lo, ZB<float>& J, ZB<float>& Y) {
+// WANT_J / WANT_Y select the basis, WANT_Z1 adds Z1 (the integral forms
+// need it, the trapezoid does not); B = int_0^x Z0 is computed only when
+// need_b (the closed form of a long interval next to this station needs it;
+// the Hermite rule of short intervals does not).
+template <bool WANT_J, bool WANT_Y, bool WANT_Z1>
+FJ_HD void eval_station_f32(float x, float p_hi, float p_lo, bool need_b, ZB<float>& J,
+                            ZB<float>& Y) {
   if (x >= 8.0f) {
     float sn, cs;
-    sincos_chi_f32(p_hi, p_lo, sn, cs);
+    sincos_cycles_f32(chi_cycles_f32(p_hi, p_lo), sn, cs);
     const float rs = rsqrt_fast(x);  // one MUFU op gives both 1/sqrt(x) and 1/x
     const float s = 8.0f * (rs * rs);
     const float z = s * s;
     const float M = kSqrt2OverPiF * rs;
+    const float sM = s * M;
     constexpr float cp0[] = FJC_F32_L_P0;
     constexpr float cq0[] = FJC_F32_L_Q0;
-    constexpr float cp1[] = FJC_F32_L_P1;
-    constexpr float cq1[] = FJC_F32_L_Q1;
     const float P0 = horner(cp0, z) * M;
-    const float Q0 = horner(cq0, z) * (s * M);
-    const float P1 = horner(cp1, z) * M;
-    const float Q1 = horner(cq1, z) * (s * M);
-    float rho0 = 0.f, rho1 = 0.f;
-    if (WANT_B) {
-      constexpr float cr0[] = FJC_F32_L_RHO0;
-      constexpr float cr1[] = FJC_F32_L_RHO1;
-      rho0 = horner(cr0, z);
-      rho1 = horner(cr1, z) * s;
+    const float Q0 = horner(cq0, z) * sM;
+    float P1 = 0.f, Q1 = 0.f;
+    if (WANT_Z1) {
+      constexpr float cp1[] = FJC_F32_L_P1;
+      constexpr float cq1[] = FJC_F32_L_Q1;
+      P1 = horner(cp1, z) * M;
+      Q1 = horner(cq1, z) * sM;
     }
     if (WANT_J) {
       J.z0 = fmaT(P0, cs, -Q0 * sn);
-      J.z1 = fmaT(P1, sn, Q1 * cs);
-      if (WANT_B) J.b = fmaT(J.z1, rho0, fmaT(-J.z0, rho1, 1.0f));
+      if (WANT_Z1) J.z1 = fmaT(P1, sn, Q1 * cs);
     }
     if (WANT_Y) {
       Y.z0 = fmaT(P0, sn, Q0 * cs);
-      Y.z1 = fmaT(Q1, sn, -P1 * cs);
-      if (WANT_B) Y.b = fmaT(Y.z1, rho0, -Y.z0 * rho1);
+      if (WANT_Z1) Y.z1 = fmaT(Q1, sn, -P1 * cs);
+    }
+    if (WANT_Z1 && need_b) {
+      constexpr float cr0[] = FJC_F32_L_RHO0;
+      constexpr float cr1[] = FJC_F32_L_RHO1;
+      const float rho0 = horner(cr0, z);
+      const float rho1 = horner(cr1, z) * s;
+      if (WANT_J) J.b = fmaT(J.z1, rho0, fmaT(-J.z0, rho1, 1.0f));
+      if (WANT_Y) Y.b = fmaT(Y.z1, rho0, -Y.z0 * rho1);
     }
   } else if (x >= 2.0f) {
     const bool hi = x >= 5.0f;
@@ -197,67 +199,86 @@ FJ_HD void eval_station_f32(float x, float p_hi, float p_lo, ZB<float>& J, ZB<fl
     if (hi) {
       if (WANT_J) {
         constexpr float c0[] = FJC_F32_S2_J0;
-        constexpr float c1[] = FJC_F32_S2_J1;
         J.z0 = horner(c0, u);
-        J.z1 = horner(c1, u);
-        if (WANT_B) {
-          constexpr float cb[] = FJC_F32_S2_BJ;
-          J.b = horner(cb, u);
+        if (WANT_Z1) {
+          constexpr float c1[] = FJC_F32_S2_J1;
+          J.z1 = horner(c1, u);
+          if (need_b) {
+            constexpr float cb[] = FJC_F32_S2_BJ;
+            J.b = horner(cb, u);
+          }
         }
       }
       if (WANT_Y) {
         constexpr float c0[] = FJC_F32_S2_Y0;
-        constexpr float c1[] = FJC_F32_S2_Y1;
         Y.z0 = horner(c0, u);
-        Y.z1 = horner(c1, u);
-        if (WANT_B) {
-          constexpr float cb[] = FJC_F32_S2_BY;
-          Y.b = horner(cb, u);
+        if (WANT_Z1) {
+          constexpr float c1[] = FJC_F32_S2_Y1;
+          Y.z1 = horner(c1, u);
+          if (need_b) {
+            constexpr float cb[] = FJC_F32_S2_BY;
+            Y.b = horner(cb, u);
+          }
         }
       }
     } else {
       if (WANT_J) {
         constexpr float c0[] = FJC_F32_S1_J0;
-        constexpr float c1[] = FJC_F32_S1_J1;
         J.z0 = horner(c0, u);
-        J.z1 = horner(c1, u);
-        if (WANT_B) {
-          constexpr float cb[] = FJC_F32_S1_BJ;
-          J.b = horner(cb, u);
+        if (WANT_Z1) {
+          constexpr float c1[] = FJC_F32_S1_J1;
+          J.z1 = horner(c1, u);
+          if (need_b) {
+            constexpr float cb[] = FJC_F32_S1_BJ;
+            J.b = horner(cb, u);
+          }
         }
       }
       if (WANT_Y) {
         constexpr float c0[] = FJC_F32_S1_Y0;
-        constexpr float c1[] = FJC_F32_S1_Y1;
         Y.z0 = horner(c0, u);
-        Y.z1 = horner(c1, u);
-        if (WANT_B) {
-          constexpr float cb[] = FJC_F32_S1_BY;
-          Y.b = horner(cb, u);
+        if (WANT_Z1) {
+          constexpr float c1[] = FJC_F32_S1_Y1;
+          Y.z1 = horner(c1, u);
+          if (need_b) {
+            constexpr float cb[] = FJC_F32_S1_BY;
+            Y.b = horner(cb, u);
+          }
         }
       }
     }
   } else {
     const float w = 0.25f * x * x;
     constexpr float ca[] = FJC_F32_S0_A;
-    constexpr float cb[] = FJC_F32_S0_B;
-    constexpr float cc[] = FJC_F32_S0_C;
     const float j0 = horner(ca, w);
-    const float j1 = x * horner(cb, w);
-    const float bj = WANT_B ? x * horner(cc, w) : 0.f;
+    float j1 = 0.f, bj = 0.f;
+    if (WANT_Z1) {
+      constexpr float cb[] = FJC_F32_S0_B;
+      j1 = x * horner(cb, w);
+      if (need_b) {
+        constexpr float cc[] = FJC_F32_S0_C;
+        bj = x * horner(cc, w);
+      }
+    }
     if (WANT_J) {
       J.z0 = j0;
-      J.z1 = j1;
-      if (WANT_B) J.b = bj;
+      if (WANT_Z1) {
+        J.z1 = j1;
+        if (need_b) J.b = bj;
+      }
     }
     if (WANT_Y) {
       constexpr float cd[] = FJC_F32_S0_D;
-      constexpr float ce[] = FJC_F32_S0_E;
-      constexpr float cf[] = FJC_F32_S0_F;
       const float L = kTwoOverPiF * log_fast(0.5f * x);
       Y.z0 = fmaT(L, j0, horner(cd, w));
-      Y.z1 = fmaT(L, j1, fmaT(x, horner(ce, w), -kTwoOverPiF * rcp_fast(x)));
-      if (WANT_B) Y.b = fmaT(L, bj, x * horner(cf, w));
+      if (WANT_Z1) {
+        constexpr float ce[] = FJC_F32_S0_E;
+        Y.z1 = fmaT(L, j1, fmaT(x, horner(ce, w), -kTwoOverPiF * rcp_fast(x)));
+        if (need_b) {
+          constexpr float cf[] = FJC_F32_S0_F;
+          Y.b = fmaT(L, bj, x * horner(cf, w));
+        }
+      }
     }
   }
 }

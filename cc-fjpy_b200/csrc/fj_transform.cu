@@ -97,14 +97,13 @@ struct Cell<float> {
     inv_k = (float)(1.0 / kd);
     inv_k2 = (float)(1.0 / (kd * kd));
   }
-  template <bool WJ, bool WY, bool WB>
-  __device__ __forceinline__ float eval(float r, ZB<float>& J, ZB<float>& Y) const {
+  template <bool WJ, bool WY, bool WZ1>
+  __device__ __forceinline__ void eval(float r, float x, bool need_b, ZB<float>& J,
+                                       ZB<float>& Y) const {
     const float p_hi = q_hi * r;
     const float e = fmaf(q_hi, r, -p_hi);
     const float p_lo = fmaf(q_lo, r, e);
-    const float x = k * r;
-    fjs::eval_station_f32<WJ, WY, WB>(x, p_hi, p_lo, J, Y);
-    return x;
+    fjs::eval_station_f32<WJ, WY, WZ1>(x, p_hi, p_lo, need_b, J, Y);
   }
 };
 template <>
@@ -116,12 +115,11 @@ struct Cell<double> {
     inv_k = 1.0 / k;
     inv_k2 = 1.0 / (k * k);
   }
-  template <bool WJ, bool WY, bool WB>
-  __device__ __forceinline__ double eval(double r, ZB<double>& J, ZB<double>& Y) const {
-    const double t = q * r;
-    const double x = k * r;
-    fjs::eval_station_f64<WJ, WY, WB>(x, t, J, Y);
-    return x;
+  template <bool WJ, bool WY, bool WZ1>
+  __device__ __forceinline__ void eval(double r, double x, bool need_b, ZB<double>& J,
+                                       ZB<double>& Y) const {
+    (void)need_b;
+    fjs::eval_station_f64<WJ, WY, WZ1>(x, q * r, J, Y);
   }
 };
 
@@ -185,19 +183,15 @@ __global__ void fj_prep_u_kernel(InDesc in, int nr, int nf, const float* __restr
 
 // ------------------------------------------------- station-amortised kernel
 template <int MODE, typename T>
-__device__ __forceinline__ void accumulate_interval(T (&acc)[2], const FjDev& a, int i, int fi,
-                                                    T scale_b, T I0J, T I1J, T I0Y, T I1Y) {
-  using MT = ModeTraits<MODE>;
-  using T2 = typename Vec2<T>::type;
-  const long long idx = (long long)i * a.nf + fi;
-  const T2 g0 = __ldg(static_cast<const T2*>(a.gb[0]) + idx);
+__device__ __forceinline__ void accumulate_interval(T (&acc)[2], const typename Vec2<T>::type& g0,
+                                                    const typename Vec2<T>::type& g1, T scale_b,
+                                                    T I0J, T I1J, T I0Y, T I1Y) {
   const T b0 = g0.y * scale_b;
   if (MODE == CCFJ_MODE_J) {
     acc[0] += fjs::fmaT(g0.x, I0J, b0 * I1J);
   } else if (MODE == CCFJ_MODE_Y) {
     acc[0] += fjs::fmaT(g0.x, I0Y, b0 * I1Y);
   } else {
-    const T2 g1 = __ldg(static_cast<const T2*>(a.gb[1]) + idx);
     const T b1 = g1.y * scale_b;
     const T J0 = fjs::fmaT(g0.x, I0J, b0 * I1J);  // J basis on input 0
     const T J1 = fjs::fmaT(g1.x, I0J, b1 * I1J);  // J basis on input 1
@@ -217,16 +211,12 @@ __device__ __forceinline__ void accumulate_interval(T (&acc)[2], const FjDev& a,
 }
 
 template <int MODE, typename T>
-__device__ __forceinline__ void accumulate_station(T (&acc)[2], const FjDev& a, int i, int fi,
-                                                   T zJ, T zY) {
-  const long long idx = (long long)i * a.nf + fi;
-  const T g0 = __ldg(static_cast<const T*>(a.gb[0]) + idx);
+__device__ __forceinline__ void accumulate_station(T (&acc)[2], T g0, T g1, T zJ, T zY) {
   if (MODE == CCFJ_MODE_J) {
     acc[0] = fjs::fmaT(g0, zJ, acc[0]);
   } else if (MODE == CCFJ_MODE_Y) {
     acc[0] = fjs::fmaT(g0, zY, acc[0]);
   } else {
-    const T g1 = __ldg(static_cast<const T*>(a.gb[1]) + idx);
     if (MODE == CCFJ_MODE_J_MINUS_Y) {
       acc[0] += g0 * zJ - g1 * zY;
     } else if (MODE == CCFJ_MODE_ABS_J) {
@@ -247,64 +237,115 @@ __device__ __forceinline__ float finish(const T (&tot)[2], T scale) {
   return sqrtf(re * re + im * im);  // np.sqrt(outr**2 + outi**2) in float32
 }
 
-template <int MODE, int ITYPE, typename T>
+// Interval (i-1, i) needs B at both of its stations when it takes the
+// closed form (see interval_moments).
+template <typename T, bool IS_Y>
+__device__ __forceinline__ bool closed_form(T dx, T x1, T tau) {
+  return fabs(dx) >= tau || (IS_Y && dx > x1);
+}
+
+// CPT cells (f, c), (f, c + 1), ... per thread share the per-station loads.
+template <int MODE, int ITYPE, typename T, int CPT>
 __global__ void __launch_bounds__(256) fj_amortized_kernel(FjDev a) {
   using MT = ModeTraits<MODE>;
   constexpr bool WJ = MT::WJ, WY = MT::WY;
   const int fi = blockIdx.x * blockDim.x + threadIdx.x;
-  const int ci = blockIdx.y * blockDim.y + threadIdx.y;
-  if (fi >= a.nf || ci >= a.nc) return;
-  Cell<T> cell;
-  cell.init(a.f[fi], a.c[ci]);
-  T tot[2] = {T(0), T(0)};
-  ZB<T> Jz, Yz;
+  const int c0 = (blockIdx.y * blockDim.y + threadIdx.y) * CPT;
+  if (fi >= a.nf || c0 >= a.nc) return;
+  Cell<T> cell[CPT];
+  const float fl = a.f[fi];
+#pragma unroll
+  for (int j = 0; j < CPT; ++j) cell[j].init(fl, a.c[min(c0 + j, a.nc - 1)]);
+  T tot[CPT][2];
+#pragma unroll
+  for (int j = 0; j < CPT; ++j) tot[j][0] = tot[j][1] = T(0);
+  ZB<T> Jz{}, Yz{};
   if (ITYPE == 1) {
     const T tau = (T)a.tau;
-    Station<T> sJp, sYp;
-    T xp = cell.template eval<WJ, WY, true>((T)__ldg(a.rs), Jz, Yz);
-    if (WJ) sJp = fjs::make_station(xp, Jz);
-    if (WY) sYp = fjs::make_station(xp, Yz);
+    Station<T> sJp[CPT], sYp[CPT];
+    T xp[CPT];
+    T r_cur = (T)__ldg(a.rs);
+    T dr_next = a.nr > 1 ? (T)__ldg(a.drs + 1) : T(0);
+#pragma unroll
+    for (int j = 0; j < CPT; ++j) {
+      xp[j] = cell[j].k * r_cur;
+      const bool nb = closed_form<T, WY>(cell[j].k * dr_next, xp[j], tau);
+      cell[j].template eval<WJ, WY, true>(r_cur, xp[j], nb, Jz, Yz);
+      if (WJ) sJp[j] = fjs::make_station(xp[j], Jz);
+      if (WY) sYp[j] = fjs::make_station(xp[j], Yz);
+    }
     for (int i0 = 1; i0 < a.nr; i0 += kChunk) {
       const int i1 = min(a.nr, i0 + kChunk);
-      T acc[2] = {T(0), T(0)};
-#pragma unroll 2
+      T acc[CPT][2];
+#pragma unroll
+      for (int j = 0; j < CPT; ++j) acc[j][0] = acc[j][1] = T(0);
       for (int i = i0; i < i1; ++i) {
         const T r = (T)__ldg(a.rs + i);
-        const T dx = cell.k * (T)__ldg(a.drs + i);
-        const T x = cell.template eval<WJ, WY, true>(r, Jz, Yz);
-        T I0J = 0, I1J = 0, I0Y = 0, I1Y = 0;
-        Station<T> sJ, sY;
-        if (WJ) {
-          sJ = fjs::make_station(x, Jz);
-          fjs::interval_moments<T, false>(sJp, sJ, dx, xp, tau, I0J, I1J);
-          sJp = sJ;
+        const T dr = dr_next;
+        dr_next = i + 1 < a.nr ? (T)__ldg(a.drs + i + 1) : T(0);
+        using T2 = typename Vec2<T>::type;
+        const long long gidx = (long long)i * a.nf + fi;
+        const T2 g0 = __ldg(static_cast<const T2*>(a.gb[0]) + gidx);
+        T2 g1;
+        if (MT::NIN > 1) g1 = __ldg(static_cast<const T2*>(a.gb[1]) + gidx);
+#pragma unroll
+        for (int j = 0; j < CPT; ++j) {
+          const T x = cell[j].k * r;
+          const T dx = cell[j].k * dr;
+          const bool nb = closed_form<T, WY>(dx, xp[j], tau) ||
+                          closed_form<T, WY>(cell[j].k * dr_next, x, tau);
+          cell[j].template eval<WJ, WY, true>(r, x, nb, Jz, Yz);
+          T I0J = 0, I1J = 0, I0Y = 0, I1Y = 0;
+          if (WJ) {
+            const Station<T> sJ = fjs::make_station(x, Jz);
+            fjs::interval_moments<T, false>(sJp[j], sJ, dx, xp[j], tau, I0J, I1J);
+            sJp[j] = sJ;
+          }
+          if (WY) {
+            const Station<T> sY = fjs::make_station(x, Yz);
+            fjs::interval_moments<T, true>(sYp[j], sY, dx, xp[j], tau, I0Y, I1Y);
+            sYp[j] = sY;
+          }
+          accumulate_interval<MODE, T>(acc[j], g0, g1, cell[j].inv_k, I0J, I1J, I0Y, I1Y);
+          xp[j] = x;
         }
-        if (WY) {
-          sY = fjs::make_station(x, Yz);
-          fjs::interval_moments<T, true>(sYp, sY, dx, xp, tau, I0Y, I1Y);
-          sYp = sY;
-        }
-        accumulate_interval<MODE, T>(acc, a, i, fi, cell.inv_k, I0J, I1J, I0Y, I1Y);
-        xp = x;
       }
-      tot[0] += acc[0];
-      tot[1] += acc[1];
+#pragma unroll
+      for (int j = 0; j < CPT; ++j) {
+        tot[j][0] += acc[j][0];
+        tot[j][1] += acc[j][1];
+      }
     }
-    a.out[(long long)ci * a.nf + fi] = finish<MODE, T>(tot, cell.inv_k2);
+#pragma unroll
+    for (int j = 0; j < CPT; ++j)
+      if (c0 + j < a.nc) a.out[(long long)(c0 + j) * a.nf + fi] = finish<MODE, T>(tot[j], cell[j].inv_k2);
   } else {
     for (int i0 = 0; i0 < a.nr; i0 += kChunk) {
       const int i1 = min(a.nr, i0 + kChunk);
-      T acc[2] = {T(0), T(0)};
-#pragma unroll 2
+      T acc[CPT][2];
+#pragma unroll
+      for (int j = 0; j < CPT; ++j) acc[j][0] = acc[j][1] = T(0);
       for (int i = i0; i < i1; ++i) {
         const T r = (T)__ldg(a.rs + i);
-        cell.template eval<WJ, WY, false>(r, Jz, Yz);
-        accumulate_station<MODE, T>(acc, a, i, fi, WJ ? Jz.z0 : T(0), WY ? Yz.z0 : T(0));
+        const long long gidx = (long long)i * a.nf + fi;
+        const T g0 = __ldg(static_cast<const T*>(a.gb[0]) + gidx);
+        T g1 = T(0);
+        if (MT::NIN > 1) g1 = __ldg(static_cast<const T*>(a.gb[1]) + gidx);
+#pragma unroll
+        for (int j = 0; j < CPT; ++j) {
+          cell[j].template eval<WJ, WY, false>(r, cell[j].k * r, false, Jz, Yz);
+          accumulate_station<MODE, T>(acc[j], g0, g1, WJ ? Jz.z0 : T(0), WY ? Yz.z0 : T(0));
+        }
       }
-      tot[0] += acc[0];
-      tot[1] += acc[1];
+#pragma unroll
+      for (int j = 0; j < CPT; ++j) {
+        tot[j][0] += acc[j][0];
+        tot[j][1] += acc[j][1];
+      }
     }
-    a.out[(long long)ci * a.nf + fi] = finish<MODE, T>(tot, T(1));
+#pragma unroll
+    for (int j = 0; j < CPT; ++j)
+      if (c0 + j < a.nc) a.out[(long long)(c0 + j) * a.nf + fi] = finish<MODE, T>(tot[j], T(1));
   }
 }
 
@@ -319,13 +360,13 @@ __device__ __forceinline__ double plain_interval(const Cell<double>& cell, doubl
                                                  double r1, double r2, double dr0) {
   ZB<double> J, Y, J2, Y2;
   if (ITYPE == 0) {
-    cell.eval<!IS_Y, IS_Y, false>(r1, J, Y);
-    cell.eval<!IS_Y, IS_Y, false>(r2, J2, Y2);
+    cell.eval<!IS_Y, IS_Y, false>(r1, cell.k * r1, false, J, Y);
+    cell.eval<!IS_Y, IS_Y, false>(r2, cell.k * r2, false, J2, Y2);
     const double z1 = IS_Y ? Y.z0 : J.z0, z2 = IS_Y ? Y2.z0 : J2.z0;
     return (g1 * z1 * r1 + g2 * z2 * r2) * dr0 * 0.5;
   }
-  cell.eval<!IS_Y, IS_Y, true>(r1, J, Y);
-  cell.eval<!IS_Y, IS_Y, true>(r2, J2, Y2);
+  cell.eval<!IS_Y, IS_Y, true>(r1, cell.k * r1, true, J, Y);
+  cell.eval<!IS_Y, IS_Y, true>(r2, cell.k * r2, true, J2, Y2);
   const ZB<double>& A = IS_Y ? Y : J;
   const ZB<double>& B = IS_Y ? Y2 : J2;
   const double k = cell.k;
@@ -418,14 +459,16 @@ __global__ void fj_normalize_kernel(float* __restrict__ out, int nc, int nf) {
 // ------------------------------------------------------------ dispatch
 namespace {
 
+constexpr int kCpt = 2;  // velocities per thread
+
 template <int MODE, typename T>
 void launch_amortized(int itype, const FjDev& d, cudaStream_t s) {
   const dim3 block(32, 8);
-  const dim3 grid(div_up(d.nf, 32), div_up(d.nc, 8));
+  const dim3 grid(div_up(d.nf, 32), div_up(d.nc, 8 * kCpt));
   if (itype == 1)
-    fj_amortized_kernel<MODE, 1, T><<<grid, block, 0, s>>>(d);
+    fj_amortized_kernel<MODE, 1, T, kCpt><<<grid, block, 0, s>>>(d);
   else
-    fj_amortized_kernel<MODE, 0, T><<<grid, block, 0, s>>>(d);
+    fj_amortized_kernel<MODE, 0, T, kCpt><<<grid, block, 0, s>>>(d);
 }
 
 template <int MODE>
@@ -691,6 +734,42 @@ CCFJ_API int FH(float* u_f, float* r, float* f, float* out, float* c, int nc, in
   return ccfj::compat(u_f, r, f, out, c, nc, nr, nf, type, CCFJ_MODE_Y);
 }
 
+namespace ccfj {
+__global__ void special_device_kernel(int precision, long long n, const double* __restrict__ x,
+                                      double* __restrict__ out) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double* o = out + 6 * i;
+  const double t = x[i] / fjs::kTwoPi;
+  if (precision == CCFJ_PREC_FP32) {
+    const float p_hi = (float)t;
+    const float p_lo = (float)(t - (double)p_hi);
+    fjs::ZB<float> J, Y;
+    fjs::eval_station_f32<true, true, true>((float)x[i], p_hi, p_lo, true, J, Y);
+    o[0] = J.z0; o[1] = J.z1; o[2] = J.b; o[3] = Y.z0; o[4] = Y.z1; o[5] = Y.b;
+  } else {
+    fjs::ZB<double> J, Y;
+    fjs::eval_station_f64<true, true, true>(x[i], t, J, Y);
+    o[0] = J.z0; o[1] = J.z1; o[2] = J.b; o[3] = Y.z0; o[4] = Y.z1; o[5] = Y.b;
+  }
+}
+}  // namespace ccfj
+
+CCFJ_API int ccfj_special_device(int precision, long long n, const double* x, double* out,
+                                 void* stream) {
+  ccfj::clear_error();
+  if (n < 0 || (n > 0 && (!x || !out)))
+    return ccfj::set_error(CCFJ_ERR_INVALID, "ccfj_special_device: bad arguments");
+  if (precision != CCFJ_PREC_FP32 && precision != CCFJ_PREC_FP64)
+    return ccfj::set_error(CCFJ_ERR_INVALID, "ccfj_special_device: bad precision %d", precision);
+  if (n == 0) return CCFJ_OK;
+  ccfj::special_device_kernel<<<ccfj::div_up(n, 256), 256, 0, (cudaStream_t)stream>>>(precision, n,
+                                                                                       x, out);
+  ccfj::count_launch();
+  CCFJ_LAUNCH_CHECK("special_device_kernel");
+  return CCFJ_OK;
+}
+
 CCFJ_API int ccfj_special_host(int precision, long long n, const double* x, double* out) {
   ccfj::clear_error();
   if (n < 0 || (n > 0 && (!x || !out)))
@@ -705,7 +784,7 @@ CCFJ_API int ccfj_special_host(int precision, long long n, const double* x, doub
       const float p_hi = (float)t;
       const float p_lo = (float)(t - (double)p_hi);
       fjs::ZB<float> J, Y;
-      fjs::eval_station_f32<true, true, true>((float)x[i], p_hi, p_lo, J, Y);
+      fjs::eval_station_f32<true, true, true>((float)x[i], p_hi, p_lo, true, J, Y);
       o[0] = J.z0; o[1] = J.z1; o[2] = J.b; o[3] = Y.z0; o[4] = Y.z1; o[5] = Y.b;
     } else {
       fjs::ZB<double> J, Y;

@@ -167,5 +167,9 @@ CCFJ_API int ccfj_set_allocator(ccfj_alloc_fn alloc, ccfj_free_fn free_fn, void 
  * precision: CCFJ_PREC_FP32 or CCFJ_PREC_FP64. For each x[i] >= 0 writes
  * out[6*i .. 6*i+5] = J0, J1, BJ, Y0, Y1, BY with BZ(x) = int_0^x Z0. */
 CCFJ_API int ccfj_special_host(int precision, long long n, const double *x, double *out);
+/* The same on the device (x, out device pointers, async on stream): the
+ * kernels' own instruction sequences, fast sine/cosine included. */
+CCFJ_API int ccfj_special_device(int precision, long long n, const double *x, double *out,
+                                 void *stream);
 
 #endif /* CCFJ_B200_H */

@@ -63,3 +63,26 @@ def test_bad_precision(lib):
     out = np.zeros(6)
     assert lib.ccfj_special_host(2, 1, x.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
                                  out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))) == 1
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec,tol", [(0, 1.5e-6), (1, None)])
+def test_device_functions(lib, prec, tol):
+    """The kernels' own code on the GPU (fast SFU sine/cosine in FP32)."""
+    import torch
+    x = torch.from_numpy(XS).cuda()
+    out = torch.zeros((len(XS), 6), dtype=torch.float64, device="cuda")
+    st = lib.ccfj_special_device(prec, len(XS), ctypes.c_void_p(x.data_ptr()),
+                                 ctypes.c_void_p(out.data_ptr()), None)
+    assert st == 0
+    torch.cuda.synchronize()
+    got = out.cpu().numpy()
+    amp = _amplitude(XS)
+    for j, name in enumerate(("J0", "J1", "BJ", "Y0", "Y1", "BY")):
+        scale = np.maximum(amp, np.abs(REF[:, j]))
+        if tol is None:
+            err = np.abs(got[:, j] - REF[:, j]) / scale / (1e-13 + 3e-16 * XS)
+            assert err.max() < 1.0, (name, err.max(), XS[err.argmax()])
+        else:
+            err = np.abs(got[:, j] - REF[:, j]) / scale
+            assert err.max() < tol, (name, err.max(), XS[err.argmax()])
