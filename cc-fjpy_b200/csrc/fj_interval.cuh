@@ -54,17 +54,14 @@ FJ_HD Station<T> make_station(T x, const ZB<T>& z) {
   return s;
 }
 
-// I0, I1 of the interval from station a (at x1) to station b (dx = x2 - x1).
-// The closed form is used for long intervals, and for the Y basis also when
-// the interval reaches close to the origin (Y0 is singular at x = 0, so the
-// Hermite rule's derivatives are not bounded there).
-template <typename T, bool IS_Y>
-FJ_HD void interval_moments(const Station<T>& a, const Station<T>& b, T dx, T x1, T tau, T& I0,
+// I0, I1 of the interval from station a (at x1) to station b (dx = x2 - x1,
+// negative for the reversed intervals of unsorted input), by the closed form
+// when `closed` (long intervals: see the kernels' closed_form) and by the
+// quintic Hermite rule otherwise.
+template <typename T>
+FJ_HD void interval_moments(const Station<T>& a, const Station<T>& b, T dx, bool closed, T& I0,
                             T& I1) {
-  // |dx|: the reference also accepts unsorted distances (reversed intervals)
-  bool use_closed = fabs(dx) >= tau;
-  if (IS_Y) use_closed = use_closed || (dx > x1);
-  if (use_closed) {
+  if (closed) {
     I0 = b.xz1 - a.xz1;
     I1 = fmaT(dx, b.xz1, (b.h - a.h) - (b.b - a.b));
   } else {

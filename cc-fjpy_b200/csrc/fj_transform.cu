@@ -21,6 +21,8 @@
 // coalesced rows and r / dr are warp-uniform broadcasts.
 #include <algorithm>
 #include <cmath>
+#include <map>
+#include <mutex>
 #include <vector>
 
 #include "ccfj_core.cuh"
@@ -237,8 +239,10 @@ __device__ __forceinline__ float finish(const T (&tot)[2], T scale) {
   return sqrtf(re * re + im * im);  // np.sqrt(outr**2 + outi**2) in float32
 }
 
-// Interval (i-1, i) needs B at both of its stations when it takes the
-// closed form (see interval_moments).
+// Whether an interval of length dx starting at x1 takes the closed form
+// (then B is needed at both of its stations): long intervals, and for the
+// Y basis (Y0 is singular at x = 0) also intervals that reach close to the
+// origin, where the Hermite rule's derivatives are not bounded.
 template <typename T, bool IS_Y>
 __device__ __forceinline__ bool closed_form(T dx, T x1, T tau) {
   return fabs(dx) >= tau || (IS_Y && dx > x1);
@@ -269,16 +273,25 @@ __global__ void __launch_bounds__(256) fj_amortized_kernel(FjDev a) {
 #pragma unroll
     for (int j = 0; j < CPT; ++j) {
       xp[j] = cell[j].k * r_cur;
-      const bool nb = closed_form<T, WY>(cell[j].k * dr_next, xp[j], tau);
+      const bool nb = closed_form<T, WY>(cell[j].k * dr_next, xp[j], tau);  // Y rule: superset
       cell[j].template eval<WJ, WY, true>(r_cur, xp[j], nb, Jz, Yz);
       if (WJ) sJp[j] = fjs::make_station(xp[j], Jz);
       if (WY) sYp[j] = fjs::make_station(xp[j], Yz);
+    }
+    // lnJ/lnY[j]: interval (i, i+1) of cell j takes the closed form in the
+    // J / Y basis (the Y rule also sends near-origin intervals there)
+    bool lnJ[CPT], lnY[CPT];
+#pragma unroll
+    for (int j = 0; j < CPT; ++j) {
+      lnJ[j] = closed_form<T, false>(cell[j].k * dr_next, xp[j], tau);
+      lnY[j] = closed_form<T, true>(cell[j].k * dr_next, xp[j], tau);
     }
     for (int i0 = 1; i0 < a.nr; i0 += kChunk) {
       const int i1 = min(a.nr, i0 + kChunk);
       T acc[CPT][2];
 #pragma unroll
       for (int j = 0; j < CPT; ++j) acc[j][0] = acc[j][1] = T(0);
+#pragma unroll 2
       for (int i = i0; i < i1; ++i) {
         const T r = (T)__ldg(a.rs + i);
         const T dr = dr_next;
@@ -292,18 +305,22 @@ __global__ void __launch_bounds__(256) fj_amortized_kernel(FjDev a) {
         for (int j = 0; j < CPT; ++j) {
           const T x = cell[j].k * r;
           const T dx = cell[j].k * dr;
-          const bool nb = closed_form<T, WY>(dx, xp[j], tau) ||
-                          closed_form<T, WY>(cell[j].k * dr_next, x, tau);
+          const bool lcJ = lnJ[j], lcY = lnY[j];
+          const T dxn = cell[j].k * dr_next;
+          if (WJ) lnJ[j] = closed_form<T, false>(dxn, x, tau);
+          if (WY) lnY[j] = closed_form<T, true>(dxn, x, tau);
+          // B is needed where an adjacent interval takes the closed form
+          const bool nb = WY ? (lcY || lnY[j]) : (lcJ || lnJ[j]);
           cell[j].template eval<WJ, WY, true>(r, x, nb, Jz, Yz);
           T I0J = 0, I1J = 0, I0Y = 0, I1Y = 0;
           if (WJ) {
             const Station<T> sJ = fjs::make_station(x, Jz);
-            fjs::interval_moments<T, false>(sJp[j], sJ, dx, xp[j], tau, I0J, I1J);
+            fjs::interval_moments<T>(sJp[j], sJ, dx, lcJ, I0J, I1J);
             sJp[j] = sJ;
           }
           if (WY) {
             const Station<T> sY = fjs::make_station(x, Yz);
-            fjs::interval_moments<T, true>(sYp[j], sY, dx, xp[j], tau, I0Y, I1Y);
+            fjs::interval_moments<T>(sYp[j], sY, dx, lcY, I0Y, I1Y);
             sYp[j] = sY;
           }
           accumulate_interval<MODE, T>(acc[j], g0, g1, cell[j].inv_k, I0J, I1J, I0Y, I1Y);
@@ -459,16 +476,30 @@ __global__ void fj_normalize_kernel(float* __restrict__ out, int nc, int nf) {
 // ------------------------------------------------------------ dispatch
 namespace {
 
-constexpr int kCpt = 2;  // velocities per thread
+// Velocities per thread of the FP32 kernel (1, 2 or 4): more share the
+// per-station loads and loop overhead, fewer keep more warps resident.
+// 0 = automatic: the tuned choice for the problem class if one is recorded
+// (ccfj_autotune_fj_v1), else 2.
+int g_force_cpt = 0;
+
+template <int MODE, typename T, int CPT>
+void launch_amortized_cpt(int itype, const FjDev& d, cudaStream_t s) {
+  const dim3 block(32, 8);
+  const dim3 grid(div_up(d.nf, 32), div_up(d.nc, 8 * CPT));
+  if (itype == 1)
+    fj_amortized_kernel<MODE, 1, T, CPT><<<grid, block, 0, s>>>(d);
+  else
+    fj_amortized_kernel<MODE, 0, T, CPT><<<grid, block, 0, s>>>(d);
+}
 
 template <int MODE, typename T>
-void launch_amortized(int itype, const FjDev& d, cudaStream_t s) {
-  const dim3 block(32, 8);
-  const dim3 grid(div_up(d.nf, 32), div_up(d.nc, 8 * kCpt));
-  if (itype == 1)
-    fj_amortized_kernel<MODE, 1, T, kCpt><<<grid, block, 0, s>>>(d);
+void launch_amortized(int itype, const FjDev& d, int cpt, cudaStream_t s) {
+  if (sizeof(T) == 8 || cpt == 1)
+    launch_amortized_cpt<MODE, T, 1>(itype, d, s);
+  else if (cpt == 4)
+    launch_amortized_cpt<MODE, T, 4>(itype, d, s);
   else
-    fj_amortized_kernel<MODE, 0, T, kCpt><<<grid, block, 0, s>>>(d);
+    launch_amortized_cpt<MODE, T, 2>(itype, d, s);
 }
 
 template <int MODE>
@@ -482,12 +513,12 @@ void launch_plain(int itype, const FjDev& d, const float* g0, const float* g1, c
 }
 
 template <int MODE>
-void launch_mode(int prec, int itype, const FjDev& d, const float* g0, const float* g1,
+void launch_mode(int prec, int itype, const FjDev& d, const float* g0, const float* g1, int cpt,
                  cudaStream_t s) {
   if (prec == CCFJ_PREC_FP32)
-    launch_amortized<MODE, float>(itype, d, s);
+    launch_amortized<MODE, float>(itype, d, cpt, s);
   else if (prec == CCFJ_PREC_FP64)
-    launch_amortized<MODE, double>(itype, d, s);
+    launch_amortized<MODE, double>(itype, d, 1, s);
   else
     launch_plain<MODE>(itype, d, g0, g1, s);
 }
@@ -495,6 +526,34 @@ void launch_mode(int prec, int itype, const FjDev& d, const float* g0, const flo
 int nin_of(int mode) { return (mode == CCFJ_MODE_J || mode == CCFJ_MODE_Y) ? 1 : 2; }
 
 }  // namespace
+
+// ------------------------------------------------------------ autotuner
+// The tuned table maps a problem class to the fastest velocities-per-thread
+// variant; classes are (mode, itype, log2 of nr, of nf, of nc).
+namespace {
+std::mutex g_tune_mu;
+std::map<long long, int> g_tune;
+
+long long tune_key(const ccfj_fj_args& a) {
+  auto lg = [](long long v) {
+    int b = 0;
+    while ((1LL << (b + 1)) <= v) ++b;
+    return (long long)b;
+  };
+  return ((((long long)a.mode * 2 + a.itype) * 64 + lg(a.nr)) * 64 + lg(a.nf)) * 64 + lg(a.nc);
+}
+}  // namespace
+
+int tuned_cpt(const ccfj_fj_args& a) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tune.find(tune_key(a));
+  return it == g_tune.end() ? 2 : it->second;
+}
+
+void record_tuned_cpt(const ccfj_fj_args& a, int cpt) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune[tune_key(a)] = cpt;
+}
 
 // Device-resident transform: every pointer in `a` is a device pointer.
 int fj_device(const ccfj_fj_args& a, cudaStream_t s) {
@@ -554,18 +613,23 @@ int fj_device(const ccfj_fj_args& a, cudaStream_t s) {
     d.gb[j] = g;
   }
 
+  const int cpt = g_force_cpt > 0 ? g_force_cpt : tuned_cpt(a);
   prof_begin(s);
   switch (a.mode) {
-    case CCFJ_MODE_J: launch_mode<CCFJ_MODE_J>(a.precision, a.itype, d, plain[0], plain[1], s); break;
-    case CCFJ_MODE_Y: launch_mode<CCFJ_MODE_Y>(a.precision, a.itype, d, plain[0], plain[1], s); break;
+    case CCFJ_MODE_J:
+      launch_mode<CCFJ_MODE_J>(a.precision, a.itype, d, plain[0], plain[1], cpt, s);
+      break;
+    case CCFJ_MODE_Y:
+      launch_mode<CCFJ_MODE_Y>(a.precision, a.itype, d, plain[0], plain[1], cpt, s);
+      break;
     case CCFJ_MODE_J_MINUS_Y:
-      launch_mode<CCFJ_MODE_J_MINUS_Y>(a.precision, a.itype, d, plain[0], plain[1], s);
+      launch_mode<CCFJ_MODE_J_MINUS_Y>(a.precision, a.itype, d, plain[0], plain[1], cpt, s);
       break;
     case CCFJ_MODE_ABS_J:
-      launch_mode<CCFJ_MODE_ABS_J>(a.precision, a.itype, d, plain[0], plain[1], s);
+      launch_mode<CCFJ_MODE_ABS_J>(a.precision, a.itype, d, plain[0], plain[1], cpt, s);
       break;
     default:
-      launch_mode<CCFJ_MODE_ABS_H>(a.precision, a.itype, d, plain[0], plain[1], s);
+      launch_mode<CCFJ_MODE_ABS_H>(a.precision, a.itype, d, plain[0], plain[1], cpt, s);
       break;
   }
   prof_end(s);
@@ -715,6 +779,56 @@ static int compat(float* u_f, float* r, float* f, float* out, float* c, int nc, 
 
 CCFJ_API int ccfj_fj_v1(const ccfj_fj_args* args, void* stream) {
   return ccfj::fj_entry(args, (cudaStream_t)stream);
+}
+
+CCFJ_API int ccfj_set_fj_variant(int cpt) {
+  if (cpt != 0 && cpt != 1 && cpt != 2 && cpt != 4)
+    return ccfj::set_error(CCFJ_ERR_INVALID, "ccfj_set_fj_variant: cpt must be 0, 1, 2 or 4");
+  ccfj::g_force_cpt = cpt;
+  return CCFJ_OK;
+}
+
+CCFJ_API int ccfj_autotune_fj_v1(const ccfj_fj_args* args, void* stream, int* best_cpt,
+                                 float* best_ms) {
+  ccfj::clear_error();
+  int st = ccfj::validate(args);
+  if (st != CCFJ_OK) return st;
+  if (!args->device_ptrs)
+    return ccfj::set_error(CCFJ_ERR_INVALID, "ccfj_autotune_fj_v1: needs device pointers");
+  cudaStream_t s = (cudaStream_t)stream;
+  const int saved = ccfj::g_force_cpt;
+  const int cands[3] = {1, 2, 4};
+  int best = 2;
+  float best_t = 1e30f;
+  cudaEvent_t e0, e1;
+  CCFJ_CUDA_TRY(cudaEventCreate(&e0));
+  CCFJ_CUDA_TRY(cudaEventCreate(&e1));
+  for (int c : cands) {
+    ccfj::g_force_cpt = c;
+    float t = 1e30f;
+    for (int rep = 0; rep < 3 && st == CCFJ_OK; ++rep) {
+      cudaEventRecord(e0, s);
+      st = ccfj::fj_device(*args, s);
+      cudaEventRecord(e1, s);
+      if (cudaEventSynchronize(e1) != cudaSuccess) st = CCFJ_ERR_CUDA;
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (rep > 0) t = std::min(t, ms);  // the first run is a warm-up
+    }
+    if (st != CCFJ_OK) break;
+    if (t < best_t) {
+      best_t = t;
+      best = c;
+    }
+  }
+  ccfj::g_force_cpt = saved;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st != CCFJ_OK) return st;
+  ccfj::record_tuned_cpt(*args, best);
+  if (best_cpt) *best_cpt = best;
+  if (best_ms) *best_ms = best_t;
+  return CCFJ_OK;
 }
 
 CCFJ_API int FJ(float* u_f, float* r, float* f, float* out, float* c, int nc, int nr, int nf,

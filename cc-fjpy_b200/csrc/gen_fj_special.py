@@ -138,7 +138,7 @@ def sample_sincos():
 
 # ---------------------------------------------------------------- fitting
 DEG = {
-    'f32': dict(S0=6, MID=10, PQ=3, RHO=5, SIN=4, COS=4),
+    'f32': dict(S0=6, MID=10, PQ=2, RHO=5, SIN=4, COS=4),
     'f64': dict(S0=13, MID=22, PQ=11, RHO=20, SIN=7, COS=8),
 }
 

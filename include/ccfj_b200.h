@@ -135,6 +135,17 @@ typedef struct ccfj_eq_args {
 
 CCFJ_API int ccfj_fj_earthquake_v1(const ccfj_eq_args *args, void *stream);
 
+/* ------------------------------------------------------------- tuning
+ * The FP32 kernels come in variants that give each thread 1, 2 or 4
+ * velocities. ccfj_autotune_fj_v1 runs every variant on the given problem
+ * (device pointers; out is overwritten), records the fastest for the
+ * problem's class (mode, itype and the powers of two of nr, nf, nc) for all
+ * later calls of this process, and returns it. ccfj_set_fj_variant(cpt)
+ * forces a variant (0 restores the tuned/default choice, which is 2). */
+CCFJ_API int ccfj_autotune_fj_v1(const ccfj_fj_args *args, void *stream, int *best_cpt,
+                                 float *best_ms);
+CCFJ_API int ccfj_set_fj_variant(int cpt);
+
 /* ------------------------------------------------------------------ misc */
 CCFJ_API const char *ccfj_last_error(void);
 CCFJ_API const char *ccfj_version(void);
