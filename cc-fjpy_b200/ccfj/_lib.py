@@ -62,6 +62,7 @@ SIGNATURES = {
     "FH": (ctypes.c_int, [_fp, _fp, _fp, _fp, _fp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                           ctypes.c_int, ctypes.c_int]),
     "ccfj_fj_v1": (ctypes.c_int, [ctypes.POINTER(FjArgs), ctypes.c_void_p]),
+    "ccfj_fj_noalloc_v1": (ctypes.c_int, [ctypes.POINTER(FjArgs), ctypes.c_void_p]),
     "ccfj_autotune_fj_v1": (ctypes.c_int, [ctypes.POINTER(FjArgs), ctypes.c_void_p,
                                            ctypes.POINTER(ctypes.c_int),
                                            ctypes.POINTER(ctypes.c_float)]),

@@ -908,3 +908,136 @@ CCFJ_API int ccfj_special_host(int precision, long long n, const double* x, doub
   }
   return CCFJ_OK;
 }
+
+// --------------------------------------------------- allocation-free entry
+// ccfj_fj_noalloc_v1 runs the same FP32 transform as ccfj_fj_v1 with device
+// pointers, but takes its scratch (pair geometry and the per-interval
+// spectrum data) from one fixed array that lives in the library's device
+// image instead of allocating it. It exists for callers that cannot
+// allocate device memory while they run: a host that has handed all free
+// device memory to its own pool allocator (so cudaMalloc/cudaMallocAsync
+// would fail or fragment it), code that must not incur the device-wide
+// synchronisation that cudaMalloc/cudaFree may cause, or code running
+// where only kernel launches on the caller's stream are allowed.
+namespace ccfj {
+
+// 16 MiB, held by every GPU that loads this library until the process exits.
+constexpr size_t kNoAllocScratchBytes = size_t(16) << 20;
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace {
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_dev_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on the current device. In host code
+// the array's name is only a host-side stand-in, so the address must come
+// from cudaGetSymbolAddress, once per device, with that device current.
+int noalloc_scratch_address(void** out) {
+  int dev = 0;
+  CCFJ_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoAllocMaxDevices)
+    return set_error(CCFJ_ERR_UNSUPPORTED, "ccfj_fj_noalloc_v1: device ordinal %d >= %d", dev,
+                     kNoAllocMaxDevices);
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_dev_ptr[dev]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || p == nullptr)
+      return set_error(CCFJ_ERR_CUDA, "ccfj_fj_noalloc_v1: cudaGetSymbolAddress failed: %s",
+                       cudaGetErrorString(e));
+    g_noalloc_dev_ptr[dev] = p;
+  }
+  *out = g_noalloc_dev_ptr[dev];
+  return CCFJ_OK;
+}
+
+size_t round256(size_t b) { return (b + 255) & ~size_t(255); }
+}  // namespace
+
+static int fj_noalloc(const ccfj_fj_args& a, cudaStream_t s) {
+  CCFJ_REQUIRE(a.device_ptrs == 1, "ccfj_fj_noalloc_v1: needs device pointers (device_ptrs = 1)");
+  if (a.precision != CCFJ_PREC_FP32)
+    return set_error(CCFJ_ERR_UNSUPPORTED, "ccfj_fj_noalloc_v1: only precision CCFJ_PREC_FP32");
+  if (a.hilbert)
+    return set_error(CCFJ_ERR_UNSUPPORTED,
+                     "ccfj_fj_noalloc_v1: hilbert = 1 is not supported; pass the transformed "
+                     "spectrum as u[1]");
+  const int nin = nin_of(a.mode);
+  const size_t geom = round256(sizeof(float) * (size_t)a.nr);
+  const size_t per_input = round256((size_t)a.nr * a.nf * (a.itype == 1 ? 8 : 4));
+  const size_t need = 2 * geom + nin * per_input;
+  if (need > kNoAllocScratchBytes)
+    return set_error(CCFJ_ERR_INVALID,
+                     "ccfj_fj_noalloc_v1: nr=%d nf=%d (%d input%s, itype %d) needs %zu bytes of "
+                     "scratch; the fixed scratch holds %zu bytes (nr*nf up to about %zu for one "
+                     "itype-1 input)",
+                     a.nr, a.nf, nin, nin > 1 ? "s" : "", a.itype, need, kNoAllocScratchBytes,
+                     (kNoAllocScratchBytes - 2 * geom) / 8);
+  void* base = nullptr;
+  int st = noalloc_scratch_address(&base);
+  if (st != CCFJ_OK) return st;
+  unsigned char* p = static_cast<unsigned char*>(base);
+  // Every scratch byte read below is first written by the preparation
+  // kernels of this call, so nothing needs clearing between calls.
+  float* drs = reinterpret_cast<float*>(p);
+  float* wtr = reinterpret_cast<float*>(p + geom);
+  fj_prep_geom_kernel<<<div_up(a.nr, 256), 256, 0, s>>>(a.r, a.nr, drs, wtr);
+  count_launch();
+  CCFJ_LAUNCH_CHECK("fj_prep_geom_kernel");
+
+  FjDev d{};
+  d.rs = a.r;
+  d.drs = drs;
+  d.f = a.f;
+  d.c = a.c;
+  d.out = a.out;
+  d.nr = a.nr;
+  d.nf = a.nf;
+  d.nc = a.nc;
+  d.tau = a.tau > 0 ? a.tau : kDefaultTau32;
+  const dim3 pb(32, 8), pg(div_up(a.nf, 32), div_up(a.nr, 8));
+  for (int j = 0; j < nin; ++j) {
+    void* g = p + 2 * geom + j * per_input;
+    const InDesc in{a.u[j], a.u_ld, (long long)a.u_es * a.fstride, a.perm};
+    fj_prep_u_kernel<float><<<pg, pb, 0, s>>>(in, a.nr, a.nf, drs, wtr, a.itype, g);
+    count_launch();
+    CCFJ_LAUNCH_CHECK("fj_prep_u_kernel");
+    d.gb[j] = g;
+  }
+  const int cpt = g_force_cpt > 0 ? g_force_cpt : tuned_cpt(a);
+  switch (a.mode) {
+    case CCFJ_MODE_J:
+      launch_mode<CCFJ_MODE_J>(a.precision, a.itype, d, nullptr, nullptr, cpt, s);
+      break;
+    case CCFJ_MODE_Y:
+      launch_mode<CCFJ_MODE_Y>(a.precision, a.itype, d, nullptr, nullptr, cpt, s);
+      break;
+    case CCFJ_MODE_J_MINUS_Y:
+      launch_mode<CCFJ_MODE_J_MINUS_Y>(a.precision, a.itype, d, nullptr, nullptr, cpt, s);
+      break;
+    case CCFJ_MODE_ABS_J:
+      launch_mode<CCFJ_MODE_ABS_J>(a.precision, a.itype, d, nullptr, nullptr, cpt, s);
+      break;
+    default:
+      launch_mode<CCFJ_MODE_ABS_H>(a.precision, a.itype, d, nullptr, nullptr, cpt, s);
+      break;
+  }
+  count_launch();
+  CCFJ_LAUNCH_CHECK("fj transform kernel");
+  if (a.normalize) {
+    fj_normalize_kernel<<<div_up(a.nf, 32), dim3(32, 8), 0, s>>>(a.out, a.nc, a.nf);
+    count_launch();
+    CCFJ_LAUNCH_CHECK("fj_normalize_kernel");
+  }
+  return CCFJ_OK;
+}
+
+}  // namespace ccfj
+
+CCFJ_API int ccfj_fj_noalloc_v1(const ccfj_fj_args* args, void* stream) {
+  ccfj::clear_error();
+  const int st = ccfj::validate(args);
+  if (st != CCFJ_OK) return st;
+  return ccfj::fj_noalloc(*args, (cudaStream_t)stream);
+}

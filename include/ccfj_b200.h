@@ -98,6 +98,30 @@ typedef struct ccfj_fj_args {
 
 CCFJ_API int ccfj_fj_v1(const ccfj_fj_args *args, void *stream);
 
+/* ------------------------------------------ allocation-free transform
+ * No counterpart in the reference. The same FP32 transform as ccfj_fj_v1
+ * with device pointers (device_ptrs = 1, precision CCFJ_PREC_FP32,
+ * hilbert = 0), for callers that cannot allocate device memory during the
+ * call: a host whose own pool allocator already holds the free device
+ * memory, or code that must avoid the device-wide synchronisation that
+ * cudaMalloc/cudaFree may cause. The caller still passes every input and the
+ * output; the call itself allocates nothing (no cudaMalloc, cudaFree or
+ * allocating library routine).
+ *
+ * Its scratch is one fixed 16 MiB array in the library's device image, which
+ * every GPU that loads the library holds until the process exits. It fits
+ * 8 * nr + (8 bytes for itype 1, 4 for itype 0) * nr * nf per input
+ * (about nr * nf <= 2.09e6 for one itype-1 input); larger problems are
+ * rejected with CCFJ_ERR_INVALID and a message giving both sizes.
+ *
+ * The first call on each device looks up the array's device address with
+ * that device current; make that first call before any stream capture.
+ * Every call uses the same array and leaves its contents behind (each call
+ * writes all the scratch it reads, so nothing is cleared): calls whose work
+ * overlaps on the GPU -- on different streams, or from different threads --
+ * race on it and must be serialised by the caller. */
+CCFJ_API int ccfj_fj_noalloc_v1(const ccfj_fj_args *args, void *stream);
+
 /* ------------------------------------------ earthquake / multi-window F-J
  * fj_earthquake (src/ccfj-gpu.pyx:270-295) and MWFJ (:297-313) from
  * time-domain traces: optional taper window, real FFT on the device, F-J of
