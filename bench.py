@@ -382,6 +382,186 @@ def run_profile_case(args):
     return 0
 
 
+# ------------------------------------------------- the other configurations
+def _dev_args(lib_, torch, nr, nf, nc, itype, mode, u_ptr, u_ld, u_es, perm_ptr, r_t, f_t, c_t,
+              out_t, u2_ptr=None, hilbert=0, ncols=None):
+    from ccfj import _lib
+    a = _lib.FjArgs()
+    a.struct_size = ctypes.sizeof(a)
+    a.nr, a.nf, a.nc = nr, nf, nc
+    a.itype, a.mode, a.precision, a.normalize, a.device_ptrs = itype, mode, 0, 1, 1
+    a.hilbert = hilbert
+    a.u[0] = u_ptr
+    a.u[1] = u2_ptr
+    a.u_ld, a.u_rows, a.u_es, a.u_ncols, a.fstride = u_ld, nr, u_es, ncols or nf, 1
+    a.perm = perm_ptr or None
+    a.r, a.f, a.c, a.out = r_t.data_ptr(), f_t.data_ptr(), c_t.data_ptr(), out_t.data_ptr()
+    return a
+
+
+def _time_device(fn, steps, warmup):
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 1e3 / steps
+
+
+def run_config(args):
+    """Device-resident timing of SURVEY configs 1, 3, 4 and 5 (one JSON line
+    each; the headline bench line is config 2)."""
+    import torch
+    import cases
+    from ccfj import _lib, _batch, _eq
+    lib = _lib.load()
+    sp = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    cfg = args.config
+    res = {"config_id": cfg, "unit": "terms/s", "dtype": "f32", "data": "synthetic (seeded)"}
+    if cfg == 1:
+        rng = np.random.default_rng(1)
+        r = np.sort(rng.uniform(1e3, 5e4, 200))
+        f = np.linspace(0.01, 1.0, 512)
+        c = np.linspace(1000, 5000, 300)
+        uf = cases.noise_spectra(rng, r, f, sigma=0.1)
+        d = {k: torch.from_numpy(v).cuda() for k, v in dict(
+            u=uf.view(np.float32), r=r.astype(np.float32), f=f.astype(np.float32),
+            c=c.astype(np.float32)).items()}
+        out = torch.empty((300, 512), device="cuda")
+        a = _dev_args(lib, torch, 200, 512, 300, 1, 0, d["u"].data_ptr(), 1024, 2, None, d["r"],
+                      d["f"], d["c"], out)
+        t = _time_device(lambda: _lib.check(lib.ccfj_fj_v1(ctypes.byref(a), sp)), args.steps,
+                         args.warmup)
+        res.update(workload="fj_noise itype=1 func=0, 200 pairs x 512 f x 300 c", seconds=t,
+                   value=200 * 512 * 300 / t)
+    elif cfg in (3, 4):
+        if cfg == 3:
+            rng = np.random.default_rng(3)
+            ntr, npts, Fs, nf, nwin = 500, 8192, 20.0, 1024, 0
+            r = np.exp(rng.uniform(np.log(1e4), np.log(2e6), ntr))
+            c = np.linspace(2000, 5000, 800)
+        else:
+            rng = np.random.default_rng(4)
+            ntr, npts, Fs, nf, nwin = 1000, 16384, 10.0, 1024, 64
+            r = np.exp(rng.uniform(np.log(5e3), np.log(1.5e6), ntr))
+            c = np.linspace(1500, 5000, 2000)
+        u = cases.ricker_records(rng, r, npts, Fs)
+        f = Fs * np.arange(nf) / npts
+        nc = len(c)
+        idx = np.argsort(r)
+        d = {k: torch.from_numpy(v).cuda() for k, v in dict(
+            u=u, perm=idx.astype(np.int64), r=r[idx].astype(np.float32), f=f.astype(np.float32),
+            c=c.astype(np.float32)).items()}
+        nw = max(nwin, 1)
+        out = torch.empty((nw, nc, nf), device="cuda")
+        a = _eq.EqArgs()
+        a.struct_size = ctypes.sizeof(a)
+        a.ntr, a.npts, a.nf, a.nc = ntr, npts, nf, nc
+        a.itype, a.func, a.precision, a.normalize, a.device_ptrs, a.fstride = 1, 0, 0, 1, 1, 1
+        a.nwin = nwin
+        a.u, a.u_ld, a.u_rows = d["u"].data_ptr(), npts, ntr
+        a.perm, a.r, a.f, a.c = d["perm"].data_ptr(), d["r"].data_ptr(), d["f"].data_ptr(), \
+            d["c"].data_ptr()
+        if nwin:
+            L = rng.integers(200, 2001, size=(nwin, ntr))
+            start = rng.integers(0, npts - L)
+            n1, n2, dl = _eq._win_params(npts, Fs, start / Fs, (start + L) / Fs, 0.9)
+            W = {k: torch.from_numpy(np.ascontiguousarray(v, dtype=np.int32)).cuda()
+                 for k, v in dict(n1=n1, n2=n2, dl=dl).items()}
+            a.win_n1, a.win_n2, a.win_delta = W["n1"].data_ptr(), W["n2"].data_ptr(), \
+                W["dl"].data_ptr()
+        a.out = out.data_ptr()
+        fn = lambda: _lib.check(lib.ccfj_fj_earthquake_v1(ctypes.byref(a), sp))  # noqa: E731
+        t = _time_device(fn, max(1, args.steps // (4 if cfg == 4 else 1)), 1)
+        terms = nw * nf * nc * ntr
+        res.update(workload=("fj_earthquake itype=1 func=0 with device rFFT, 500 traces x 8192 "
+                             "samples, nf=1024 bins, nc=800" if cfg == 3 else
+                             "MWFJ itype=1 func=0, 1000 traces x 16384 samples, 64 windows, "
+                             "nf=1024, nc=2000"), seconds=t, value=terms / t)
+    elif cfg == 5:
+        rng = np.random.default_rng(5)
+        nsets, nf, nc = 512, 1024, 500
+        counts = np.exp(rng.uniform(np.log(50), np.log(20000), nsets)).astype(np.int64)
+        off = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+        total = int(off[-1])
+        f = np.linspace(0.01, 1.0, nf)
+        c = np.linspace(1000, 5000, nc)
+        # spectra generated on the device (14 GB as complex64): c(f) law with
+        # an overtone and sigma = 0.2 noise, as the large-array workload
+        g = torch.Generator(device="cuda").manual_seed(5)
+        r_t = (torch.rand(total, generator=g, device="cuda", dtype=torch.float64) * 299.5e3 + 500.0)
+        f_t = torch.from_numpy(f).cuda()
+        cf = 2000.0 + 1500.0 * torch.exp(-f_t / 0.2)
+        U = torch.empty((total, 2 * nf), dtype=torch.float32, device="cuda")
+        for s0 in range(0, total, 65536):
+            rr = r_t[s0:s0 + 65536, None]
+            ph = 2 * np.pi * f_t[None, :] * rr
+            re = torch.special.bessel_j0(ph / cf) + 0.5 * torch.special.bessel_j0(ph / (cf + 800))
+            n = rr.shape[0]
+            U[s0:s0 + n, 0::2] = (re + 0.2 * torch.randn(n, nf, generator=g, device="cuda",
+                                                        dtype=torch.float64)).float()
+            U[s0:s0 + n, 1::2] = (0.2 * torch.randn(n, nf, generator=g, device="cuda",
+                                                   dtype=torch.float64)).float()
+        r_sorted = torch.empty(total, dtype=torch.float32, device="cuda")
+        perm = torch.empty(total, dtype=torch.int64, device="cuda")
+        for b in range(nsets):
+            seg = r_t[off[b]:off[b + 1]]
+            srt, ix = torch.sort(seg, stable=True)
+            r_sorted[off[b]:off[b + 1]] = srt.float()
+            perm[off[b]:off[b + 1]] = ix + int(off[b])
+        d_off = torch.from_numpy(off).cuda()
+        f32 = torch.from_numpy(f.astype(np.float32)).cuda()
+        c32 = torch.from_numpy(c.astype(np.float32)).cuda()
+        out = torch.empty((nsets, nc, nf), device="cuda")
+        ba = _batch.BatchArgs()
+        ba.struct_size = ctypes.sizeof(ba)
+        ba.nsets, ba.nf, ba.nc = nsets, nf, nc
+        ba.itype, ba.mode, ba.precision, ba.normalize, ba.device_ptrs = 1, 0, 0, 1, 1
+        ba.use_graph = 1
+        ba.offsets, ba.total_pairs = d_off.data_ptr(), total
+        ba.r, ba.u[0] = r_sorted.data_ptr(), U.data_ptr()
+        ba.u_ld, ba.u_rows, ba.u_es, ba.u_ncols, ba.fstride = 2 * nf, total, 2, nf, 1
+        ba.perm, ba.f, ba.c, ba.out = perm.data_ptr(), f32.data_ptr(), c32.data_ptr(), \
+            out.data_ptr()
+        s_cap = torch.cuda.Stream()
+        spc = ctypes.c_void_p(s_cap.cuda_stream)
+
+        def batch_step():
+            _lib.check(lib.ccfj_fj_batch_v1(ctypes.byref(ba), spc))
+
+        with torch.cuda.stream(s_cap):
+            t_batch = _time_device(batch_step, 2, 1)
+        lib.ccfj_batch_graph_cache_clear()
+        # the same work as 512 separate transforms
+        single = []
+        for b in range(nsets):
+            o = int(off[b])
+            n = int(counts[b])
+            single.append(_dev_args(lib, torch, n, nf, nc, 1, 0, U.data_ptr(), 2 * nf, 2,
+                                    perm.data_ptr() + 8 * o, r_sorted[o:o + n], f32, c32,
+                                    out[b]))
+            single[-1].u_rows = total
+
+        def separate():
+            for a in single:
+                _lib.check(lib.ccfj_fj_v1(ctypes.byref(a), sp))
+
+        t_sep = _time_device(separate, 1, 1)
+        terms = total * nf * nc
+        res.update(workload="512 subarrays, %d pairs in total (log-uniform 50-20000 each), "
+                            "nf=1024, nc=500, itype=1 func=0; one persistent graph-replayed "
+                            "launch" % total, seconds=t_batch, value=terms / t_batch,
+                   separate_launches_seconds=t_sep, separate_launches_value=terms / t_sep,
+                   speedup_vs_separate=t_sep / t_batch)
+    print(json.dumps(res))
+    return 0
+
+
 def _quiet(fn, *a, **k):
     with warnings.catch_warnings():
         warnings.simplefilter("ignore")
@@ -397,7 +577,11 @@ def main():
     ap.add_argument("--profile-case", action="store_true",
                     help="run only the device transform on a 512-frequency slice of the workload "
                          "(steps launches, no extras): the case the ncu captures use")
+    ap.add_argument("--config", type=int, default=0, choices=(0, 1, 3, 4, 5),
+                    help="time another SURVEY configuration (device-resident; one JSON line)")
     args = ap.parse_args()
+    if args.config:
+        return run_config(args)
     if args.profile_case:
         return run_profile_case(args)
     rank = int(os.environ.get("RANK", "0"))

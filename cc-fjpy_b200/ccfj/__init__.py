@@ -28,7 +28,7 @@ from . import _lib
 from ._lib import CcfjError  # noqa: F401
 
 __all__ = ["fj_noise", "fj_earthquake", "MWFJ", "fj", "fhr", "fhi", "fh", "win",
-           "GetStationPairs", "CC", "CcfjError"]
+           "GetStationPairs", "CC", "CcfjError", "fj_noise_batch"]
 
 _FUNC_MSG = "set func as 0 for Bessel function 1 for Hankel function"
 
@@ -234,3 +234,4 @@ def CC(*args, **kwargs):
 
 
 from ._eq import fj_earthquake, MWFJ  # noqa: E402
+from ._batch import fj_noise_batch  # noqa: E402

@@ -69,6 +69,11 @@ void dev_free(void* p, cudaStream_t s) {
   cudaFreeAsync(p, s);
 }
 
+bool allocator_hooked() {
+  std::lock_guard<std::mutex> lk(g_alloc_mu);
+  return g_alloc != nullptr;
+}
+
 Scratch::~Scratch() {
   for (int i = n_ - 1; i >= 0; --i) dev_free(ptrs_[i], s_);
 }

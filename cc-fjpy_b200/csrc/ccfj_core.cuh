@@ -27,6 +27,8 @@ void clear_error();
 // cudaMallocAsync / cudaFreeAsync are used.
 void* dev_alloc(size_t bytes, cudaStream_t s);
 void dev_free(void* p, cudaStream_t s);
+// True when ccfj_set_allocator installed a caller allocator.
+bool allocator_hooked();
 
 // A scope that frees everything it allocated, in reverse order, on the
 // stream it was created with.

@@ -1,0 +1,485 @@
+// Ragged batch: many data sets (subarrays) of uneven pair counts that share
+// the frequency and velocity grids, transformed in one persistent launch.
+//
+// The reference has no batch entry; a user calls fj_noise once per subarray
+// (src/ccfj-gpu.pyx:241-268), and each call pays its own allocation, copies
+// and launch. Here the pairs of all sets are concatenated (CSR offsets), the
+// preparation runs once over all of them, and one persistent kernel with
+// one CTA per resident slot pulls work items -- (set, 32 frequencies, 8*CPT
+// velocities) -- from a global atomic counter, largest sets first (a
+// longest-processing-time order, so the uneven costs even out at the end).
+// The counter is only incremented: no thread ever waits on another.
+//
+// With use_graph, the whole sequence (counter reset, preparation, Hilbert
+// transform, persistent kernel, normalisation, and its stream-ordered
+// scratch allocations) is captured once per argument set into a CUDA graph
+// and replayed on later calls.
+#include <algorithm>
+#include <climits>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+
+#include "fj_cells.cuh"
+
+namespace ccfj {
+
+namespace {
+
+__device__ __forceinline__ int set_of(const long long* __restrict__ off, int nsets, long long i) {
+  int lo = 0, hi = nsets;  // off[lo] <= i < off[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (off[mid] <= i)
+      lo = mid;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+__global__ void batch_prep_geom_kernel(const float* __restrict__ rs,
+                                       const long long* __restrict__ off, int nsets,
+                                       long long total, float* __restrict__ drs,
+                                       float* __restrict__ wtr) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  const int b = set_of(off, nsets, i);
+  const long long s = off[b], e = off[b + 1];
+  const float r = rs[i];
+  const float dl = i > s ? r - rs[i - 1] : 0.0f;
+  const float dr = i + 1 < e ? rs[i + 1] - r : 0.0f;
+  drs[i] = dl;
+  const float w0 = i > s ? fmaxf(dl, 0.1f) : 0.0f;
+  const float w1 = i + 1 < e ? fmaxf(dr, 0.1f) : 0.0f;
+  wtr[i] = (w0 + w1) * 0.5f * r;
+}
+
+// As fj_prep_u_kernel, with the interval data of each set's first pair zero.
+__global__ void batch_prep_u_kernel(InDesc in, const long long* __restrict__ off, int nsets,
+                                    long long total, int nf, const float* __restrict__ drs,
+                                    const float* __restrict__ wtr, int itype,
+                                    void* __restrict__ dst) {
+  // rows on grid x (up to 2^31 - 1 blocks), frequencies on grid y
+  const int fi = blockIdx.y * blockDim.x + threadIdx.x;
+  const long long i = (long long)blockIdx.x * blockDim.y + threadIdx.y;
+  if (fi >= nf || i >= total) return;
+  const long long row = in.perm ? in.perm[i] : i;
+  const float g = in.p[row * in.ld + (long long)fi * in.cs];
+  if (itype == 1) {
+    float2 v = make_float2(0.f, 0.f);
+    const int b = set_of(off, nsets, i);
+    if (i > off[b]) {
+      const long long rowp = in.perm ? in.perm[i - 1] : i - 1;
+      const float gp = in.p[rowp * in.ld + (long long)fi * in.cs];
+      v = make_float2(gp, (g - gp) / fmaxf(drs[i], 0.1f));
+    }
+    static_cast<float2*>(dst)[i * nf + fi] = v;
+  } else {
+    static_cast<float*>(dst)[i * nf + fi] = g * wtr[i];
+  }
+}
+
+// Sets ordered by pair count, largest first (one CTA; nsets <= 4096).
+constexpr int kSortMax = 4096;
+__global__ void batch_order_kernel(const long long* __restrict__ off, int nsets,
+                                   int* __restrict__ order) {
+  __shared__ long long key[kSortMax];
+  __shared__ int val[kSortMax];
+  int n2 = 1;
+  while (n2 < nsets) n2 <<= 1;
+  for (int t = threadIdx.x; t < n2; t += blockDim.x) {
+    key[t] = t < nsets ? -(off[t + 1] - off[t]) : LLONG_MAX;  // ascending key = descending size
+    val[t] = t;
+  }
+  __syncthreads();
+  for (int k = 2; k <= n2; k <<= 1) {       // bitonic sort of (key, val)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int t = threadIdx.x; t < n2; t += blockDim.x) {
+        const int p = t ^ j;
+        if (p > t) {
+          const bool up = (t & k) == 0;
+          const bool gt = key[t] > key[p] || (key[t] == key[p] && val[t] > val[p]);
+          if (gt == up) {
+            const long long tk = key[t];
+            key[t] = key[p];
+            key[p] = tk;
+            const int tv = val[t];
+            val[t] = val[p];
+            val[p] = tv;
+          }
+        }
+      }
+      __syncthreads();
+    }
+  }
+  for (int t = threadIdx.x; t < nsets; t += blockDim.x) order[t] = val[t];
+}
+
+__global__ void batch_identity_order_kernel(int nsets, int* __restrict__ order) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t < nsets) order[t] = t;
+}
+
+struct BatchDev {
+  FjDev base;                 // shared arrays for all sets; nr unused
+  const long long* off;
+  const int* order;
+  int nsets;
+  int ftiles, ctiles;
+  long long items;
+  unsigned long long* counter;
+};
+
+template <int MODE, int ITYPE, int CPT>
+__global__ void __launch_bounds__(256) fj_batch_persistent_kernel(BatchDev bd) {
+  __shared__ long long item_s;
+  using T2 = float2;
+  for (;;) {
+    if (threadIdx.x == 0 && threadIdx.y == 0) item_s = (long long)atomicAdd(bd.counter, 1ULL);
+    __syncthreads();
+    const long long item = item_s;
+    __syncthreads();  // all threads hold `item` before thread 0 may overwrite item_s
+    if (item >= bd.items) break;
+    const long long per_set = (long long)bd.ftiles * bd.ctiles;
+    const int b = bd.order[item / per_set];
+    const int rem = (int)(item % per_set);
+    const long long o = bd.off[b];
+    FjDev a = bd.base;
+    a.nr = (int)(bd.off[b + 1] - o);
+    a.rs += o;
+    a.drs += o;
+    constexpr long long esz = ITYPE == 1 ? sizeof(T2) : sizeof(float);
+    a.gb[0] = static_cast<const char*>(bd.base.gb[0]) + o * a.nf * esz;
+    if (ModeTraits<MODE>::NIN > 1) a.gb[1] = static_cast<const char*>(bd.base.gb[1]) + o * a.nf * esz;
+    a.out += (long long)b * a.nc * a.nf;
+    const int fi = (rem % bd.ftiles) * 32 + threadIdx.x;
+    const int c0 = ((rem / bd.ftiles) * 8 + threadIdx.y) * CPT;
+    fj_cells<MODE, ITYPE, float, CPT>(a, fi, c0);
+  }
+}
+
+// Per (set, frequency) column normalisation (builtin-max semantics, as
+// fj_normalize_kernel), set = blockIdx.y.
+__global__ void batch_normalize_kernel(float* __restrict__ out, int nc, int nf) {
+  __shared__ float red[8][33];
+  __shared__ float colmax[32];
+  float* o = out + (long long)blockIdx.y * nc * nf;
+  const int fi = blockIdx.x * 32 + threadIdx.x;
+  float m = -INFINITY;
+  if (fi < nf)
+    for (int c = threadIdx.y; c < nc; c += blockDim.y) m = fmaxf(m, fabsf(o[(long long)c * nf + fi]));
+  red[threadIdx.y][threadIdx.x] = m;
+  __syncthreads();
+  if (threadIdx.y == 0) {
+    for (int y = 1; y < (int)blockDim.y; ++y) m = fmaxf(m, red[y][threadIdx.x]);
+    if (fi < nf) {
+      const float first = fabsf(o[fi]);
+      colmax[threadIdx.x] = isnan(first) ? first : m;
+    }
+  }
+  __syncthreads();
+  if (fi < nf) {
+    const float dv = colmax[threadIdx.x];
+    for (int c = threadIdx.y; c < nc; c += blockDim.y) {
+      const long long k = (long long)c * nf + fi;
+      o[k] = o[k] / dv;
+    }
+  }
+}
+
+int nin_of_mode(int mode) { return (mode == CCFJ_MODE_J || mode == CCFJ_MODE_Y) ? 1 : 2; }
+
+template <int MODE, int CPT>
+void launch_batch_cpt(int itype, const BatchDev& bd, int grid, cudaStream_t s) {
+  if (itype == 1)
+    fj_batch_persistent_kernel<MODE, 1, CPT><<<grid, dim3(32, 8), 0, s>>>(bd);
+  else
+    fj_batch_persistent_kernel<MODE, 0, CPT><<<grid, dim3(32, 8), 0, s>>>(bd);
+}
+
+template <int MODE>
+int launch_batch(int itype, int cpt, BatchDev bd, cudaStream_t s) {
+  int dev = 0, sms = 0, per_sm = 0;
+  CCFJ_CUDA_TRY(cudaGetDevice(&dev));
+  CCFJ_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const void* fn = nullptr;
+#define CCFJ_PICK(C)                                                                           \
+  fn = itype == 1 ? (const void*)fj_batch_persistent_kernel<MODE, 1, C>                        \
+                  : (const void*)fj_batch_persistent_kernel<MODE, 0, C>
+  if (cpt == 1)
+    CCFJ_PICK(1);
+  else if (cpt == 4)
+    CCFJ_PICK(4);
+  else
+    CCFJ_PICK(2);
+#undef CCFJ_PICK
+  CCFJ_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, 0));
+  const long long slots = (long long)sms * (per_sm > 0 ? per_sm : 1);
+  const int grid = (int)(bd.items < slots ? bd.items : slots);
+  if (cpt == 1)
+    launch_batch_cpt<MODE, 1>(itype, bd, grid, s);
+  else if (cpt == 4)
+    launch_batch_cpt<MODE, 4>(itype, bd, grid, s);
+  else
+    launch_batch_cpt<MODE, 2>(itype, bd, grid, s);
+  return CCFJ_OK;
+}
+
+int batch_validate(const ccfj_batch_args* a) {
+  CCFJ_REQUIRE(a != nullptr, "ccfj_fj_batch_v1: args is NULL");
+  CCFJ_REQUIRE(a->struct_size == (int)sizeof(ccfj_batch_args),
+               "ccfj_fj_batch_v1: struct_size %d != %d (header mismatch)", a->struct_size,
+               (int)sizeof(ccfj_batch_args));
+  CCFJ_REQUIRE(a->nsets >= 1 && a->nf >= 1 && a->nc >= 1,
+               "ccfj_fj_batch_v1: nsets=%d nf=%d nc=%d must be >= 1", a->nsets, a->nf, a->nc);
+  CCFJ_REQUIRE(a->nsets <= 65535, "ccfj_fj_batch_v1: nsets=%d > 65535", a->nsets);
+  CCFJ_REQUIRE(a->itype == 0 || a->itype == 1, "ccfj_fj_batch_v1: itype must be 0 or 1");
+  CCFJ_REQUIRE(a->mode >= CCFJ_MODE_J && a->mode <= CCFJ_MODE_ABS_H, "ccfj_fj_batch_v1: bad mode");
+  CCFJ_REQUIRE(a->precision == CCFJ_PREC_FP32, "ccfj_fj_batch_v1: only CCFJ_PREC_FP32");
+  CCFJ_REQUIRE(a->variant == 0 || a->variant == 1 || a->variant == 2 || a->variant == 4,
+               "ccfj_fj_batch_v1: variant must be 0, 1, 2 or 4");
+  CCFJ_REQUIRE(a->offsets && a->r && a->f && a->c && a->out && a->u[0],
+               "ccfj_fj_batch_v1: NULL array");
+  CCFJ_REQUIRE(a->fstride >= 1 && a->u_es >= 1 && a->u_ld >= 1, "ccfj_fj_batch_v1: bad layout");
+  CCFJ_REQUIRE(a->u_ncols >= 1 && (a->u_ncols + a->fstride - 1) / a->fstride == a->nf,
+               "ccfj_fj_batch_v1: %d columns with fstride %d do not give nf=%d", a->u_ncols,
+               a->fstride, a->nf);
+  CCFJ_REQUIRE(a->u_ld >= (long long)(a->u_ncols - 1) * a->u_es + 1, "ccfj_fj_batch_v1: u_ld too small");
+  if (a->hilbert)
+    CCFJ_REQUIRE(a->mode == CCFJ_MODE_J_MINUS_Y && a->u[1] == nullptr,
+                 "ccfj_fj_batch_v1: hilbert=1 needs mode J_MINUS_Y and u[1] == NULL");
+  else
+    CCFJ_REQUIRE(nin_of_mode(a->mode) == 1 || a->u[1], "ccfj_fj_batch_v1: mode needs two inputs");
+  return CCFJ_OK;
+}
+
+// The device sequence of one batch (all pointers device pointers;
+// `total` = offsets[nsets], known to the caller).
+int batch_device(const ccfj_batch_args& a, long long total, cudaStream_t s) {
+  Scratch sc(s);
+  const int nin = nin_of_mode(a.mode);
+  float* drs = sc.get_n<float>(total);
+  float* wtr = sc.get_n<float>(total);
+  int* order = sc.get_n<int>(a.nsets);
+  unsigned long long* counter = sc.get_n<unsigned long long>(1);
+  if (!drs || !wtr || !order || !counter) return CCFJ_ERR_ALLOC;
+  CCFJ_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s));
+  if (a.nsets <= kSortMax)
+    batch_order_kernel<<<1, 1024, 0, s>>>(a.offsets, a.nsets, order);
+  else
+    batch_identity_order_kernel<<<div_up(a.nsets, 256), 256, 0, s>>>(a.nsets, order);
+  count_launch();
+  CCFJ_LAUNCH_CHECK("batch_order_kernel");
+  batch_prep_geom_kernel<<<div_up(total, 256), 256, 0, s>>>(a.r, a.offsets, a.nsets, total, drs,
+                                                             wtr);
+  count_launch();
+  CCFJ_LAUNCH_CHECK("batch_prep_geom_kernel");
+
+  InDesc in[2];
+  for (int j = 0; j < 2; ++j) in[j] = InDesc{a.u[j], a.u_ld, (long long)a.u_es * a.fstride, a.perm};
+  if (a.hilbert) {
+    float* hb = sc.get_n<float>((size_t)total * a.nf);
+    if (!hb) return CCFJ_ERR_ALLOC;
+    CCFJ_REQUIRE(total <= INT_MAX, "ccfj_fj_batch_v1: too many pairs for the Hilbert transform");
+    const int st = hilbert_rows(InDesc{a.u[0], a.u_ld, a.u_es, a.perm}, a.u_ncols, a.u_es,
+                                (int)total, a.nf, a.fstride, hb, s, sc);
+    if (st != CCFJ_OK) return st;
+    in[1] = InDesc{hb, a.nf, 1, nullptr};
+  }
+  BatchDev bd{};
+  const size_t esz = a.itype == 1 ? 8 : 4;
+  for (int j = 0; j < nin; ++j) {
+    void* g = sc.get((size_t)total * a.nf * esz);
+    if (!g) return CCFJ_ERR_ALLOC;
+    batch_prep_u_kernel<<<dim3(div_up(total, 8), div_up(a.nf, 32)), dim3(32, 8), 0, s>>>(
+        in[j], a.offsets, a.nsets, total, a.nf, drs, wtr, a.itype, g);
+    count_launch();
+    CCFJ_LAUNCH_CHECK("batch_prep_u_kernel");
+    bd.base.gb[j] = g;
+  }
+  bd.base.rs = a.r;
+  bd.base.drs = drs;
+  bd.base.f = a.f;
+  bd.base.c = a.c;
+  bd.base.out = a.out;
+  bd.base.nf = a.nf;
+  bd.base.nc = a.nc;
+  bd.base.tau = a.tau > 0 ? a.tau : kDefaultTau32;
+  bd.off = a.offsets;
+  bd.order = order;
+  bd.nsets = a.nsets;
+  const int cpt = a.variant > 0 ? a.variant : 2;
+  bd.ftiles = div_up(a.nf, 32);
+  bd.ctiles = div_up(a.nc, 8 * cpt);
+  bd.items = (long long)a.nsets * bd.ftiles * bd.ctiles;
+  bd.counter = counter;
+  int st = CCFJ_OK;
+  switch (a.mode) {
+    case CCFJ_MODE_J: st = launch_batch<CCFJ_MODE_J>(a.itype, cpt, bd, s); break;
+    case CCFJ_MODE_Y: st = launch_batch<CCFJ_MODE_Y>(a.itype, cpt, bd, s); break;
+    case CCFJ_MODE_J_MINUS_Y: st = launch_batch<CCFJ_MODE_J_MINUS_Y>(a.itype, cpt, bd, s); break;
+    case CCFJ_MODE_ABS_J: st = launch_batch<CCFJ_MODE_ABS_J>(a.itype, cpt, bd, s); break;
+    default: st = launch_batch<CCFJ_MODE_ABS_H>(a.itype, cpt, bd, s); break;
+  }
+  if (st != CCFJ_OK) return st;
+  count_launch();
+  CCFJ_LAUNCH_CHECK("fj_batch_persistent_kernel");
+  if (a.normalize) {
+    batch_normalize_kernel<<<dim3(div_up(a.nf, 32), a.nsets), dim3(32, 8), 0, s>>>(a.out, a.nc,
+                                                                                   a.nf);
+    count_launch();
+    CCFJ_LAUNCH_CHECK("batch_normalize_kernel");
+  }
+  return CCFJ_OK;
+}
+
+// ---------------------------------------------------------- graph cache
+struct GraphEntry {
+  cudaGraphExec_t exec = nullptr;
+};
+std::mutex g_graph_mu;
+std::map<std::string, GraphEntry> g_graphs;
+cudaStream_t g_capture_stream[64] = {};
+
+std::string graph_key(const ccfj_batch_args& a, long long total) {
+  std::string k(reinterpret_cast<const char*>(&a), sizeof(a));
+  k.append(reinterpret_cast<const char*>(&total), sizeof(total));
+  int dev = 0;
+  cudaGetDevice(&dev);
+  k.append(reinterpret_cast<const char*>(&dev), sizeof(dev));
+  return k;
+}
+
+int batch_device_graph(const ccfj_batch_args& a, long long total, cudaStream_t s) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (s) CCFJ_CUDA_TRY(cudaStreamIsCapturing(s, &cs));
+  if (cs != cudaStreamCaptureStatusNone) return batch_device(a, total, s);  // caller's capture
+  const std::string key = graph_key(a, total);
+  std::lock_guard<std::mutex> lk(g_graph_mu);
+  auto it = g_graphs.find(key);
+  if (it == g_graphs.end()) {
+    int dev = 0;
+    CCFJ_CUDA_TRY(cudaGetDevice(&dev));
+    CCFJ_REQUIRE(dev >= 0 && dev < 64, "ccfj_fj_batch_v1: device ordinal %d", dev);
+    cudaStream_t cap = s;
+    if (!cap) {  // the legacy default stream cannot be captured
+      if (!g_capture_stream[dev])
+        CCFJ_CUDA_TRY(cudaStreamCreateWithFlags(&g_capture_stream[dev], cudaStreamNonBlocking));
+      cap = g_capture_stream[dev];
+    }
+    cudaGraph_t graph = nullptr;
+    CCFJ_CUDA_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
+    const int st = batch_device(a, total, cap);
+    const cudaError_t e = cudaStreamEndCapture(cap, &graph);
+    if (st != CCFJ_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      return st;
+    }
+    if (e != cudaSuccess)
+      return set_error(CCFJ_ERR_CUDA, "ccfj_fj_batch_v1: graph capture failed: %s",
+                       cudaGetErrorString(e));
+    GraphEntry ge;
+    const cudaError_t ei = cudaGraphInstantiate(&ge.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ei != cudaSuccess)
+      return set_error(CCFJ_ERR_CUDA, "ccfj_fj_batch_v1: graph instantiation failed: %s",
+                       cudaGetErrorString(ei));
+    it = g_graphs.emplace(key, ge).first;
+  }
+  if (s) {
+    CCFJ_CUDA_TRY(cudaGraphLaunch(it->second.exec, s));
+  } else {
+    int dev = 0;
+    CCFJ_CUDA_TRY(cudaGetDevice(&dev));
+    cudaStream_t cap = g_capture_stream[dev];
+    CCFJ_CUDA_TRY(cudaGraphLaunch(it->second.exec, cap));
+    CCFJ_CUDA_TRY(cudaStreamSynchronize(cap));
+  }
+  count_launch();
+  return CCFJ_OK;
+}
+
+int batch_run_device(const ccfj_batch_args& a, long long total, cudaStream_t s) {
+  if (a.use_graph && !allocator_hooked()) return batch_device_graph(a, total, s);
+  return batch_device(a, total, s);
+}
+
+int batch_host(const ccfj_batch_args& a, cudaStream_t s) {
+  const long long* off = a.offsets;
+  CCFJ_REQUIRE(off[0] == 0, "ccfj_fj_batch_v1: offsets[0] must be 0");
+  for (int b = 0; b < a.nsets; ++b)
+    CCFJ_REQUIRE(off[b + 1] > off[b], "ccfj_fj_batch_v1: set %d is empty or offsets decrease", b);
+  const long long total = off[a.nsets];
+  CCFJ_REQUIRE(a.total_pairs == 0 || a.total_pairs == total,
+               "ccfj_fj_batch_v1: total_pairs %lld != offsets[nsets] %lld", a.total_pairs, total);
+  CCFJ_REQUIRE(a.u_rows >= total || a.perm, "ccfj_fj_batch_v1: u_rows < total pairs");
+  if (a.perm)
+    for (long long i = 0; i < total; ++i)
+      CCFJ_REQUIRE(a.perm[i] >= 0 && a.perm[i] < a.u_rows, "ccfj_fj_batch_v1: perm[%lld] out of range",
+                   i);
+  const int nin = a.hilbert ? 1 : nin_of_mode(a.mode);
+  const long long span = (a.u_rows - 1) * a.u_ld + (long long)(a.u_ncols - 1) * a.u_es + 1;
+  const float* lo = a.u[0];
+  const float* hi = a.u[0] + span;
+  if (nin == 2) {
+    lo = std::min(lo, a.u[1]);
+    hi = std::max(hi, a.u[1] + span);
+  }
+  CCFJ_REQUIRE(nin == 1 || (size_t)(hi - lo) <= (size_t)(2 * span + 16),
+               "ccfj_fj_batch_v1: host mode needs both inputs in one array (real/imaginary parts)");
+  Scratch sc(s);
+  float* du = sc.get_n<float>(hi - lo);
+  long long* doff = sc.get_n<long long>(a.nsets + 1);
+  float* dr = sc.get_n<float>(total);
+  float* df = sc.get_n<float>(a.nf);
+  float* dc = sc.get_n<float>(a.nc);
+  float* dout = sc.get_n<float>((size_t)a.nsets * a.nc * a.nf);
+  long long* dp = a.perm ? sc.get_n<long long>(total) : nullptr;
+  if (!du || !doff || !dr || !df || !dc || !dout || (a.perm && !dp)) return CCFJ_ERR_ALLOC;
+  CCFJ_CUDA_TRY(cudaMemcpyAsync(du, lo, sizeof(float) * (hi - lo), cudaMemcpyHostToDevice, s));
+  CCFJ_CUDA_TRY(cudaMemcpyAsync(doff, off, sizeof(long long) * (a.nsets + 1), cudaMemcpyHostToDevice, s));
+  CCFJ_CUDA_TRY(cudaMemcpyAsync(dr, a.r, sizeof(float) * total, cudaMemcpyHostToDevice, s));
+  CCFJ_CUDA_TRY(cudaMemcpyAsync(df, a.f, sizeof(float) * a.nf, cudaMemcpyHostToDevice, s));
+  CCFJ_CUDA_TRY(cudaMemcpyAsync(dc, a.c, sizeof(float) * a.nc, cudaMemcpyHostToDevice, s));
+  if (dp) CCFJ_CUDA_TRY(cudaMemcpyAsync(dp, a.perm, sizeof(long long) * total, cudaMemcpyHostToDevice, s));
+  ccfj_batch_args d = a;
+  d.device_ptrs = 1;
+  d.use_graph = 0;  // per-call buffers: nothing to replay
+  for (int j = 0; j < nin; ++j) d.u[j] = du + (a.u[j] - lo);
+  d.offsets = doff;
+  d.r = dr;
+  d.f = df;
+  d.c = dc;
+  d.out = dout;
+  d.perm = dp;
+  int st = batch_device(d, total, s);
+  if (st != CCFJ_OK) return st;
+  CCFJ_CUDA_TRY(cudaMemcpyAsync(a.out, dout, sizeof(float) * a.nsets * a.nc * a.nf,
+                                cudaMemcpyDeviceToHost, s));
+  CCFJ_CUDA_TRY(cudaStreamSynchronize(s));
+  return CCFJ_OK;
+}
+
+}  // namespace
+
+}  // namespace ccfj
+
+CCFJ_API int ccfj_fj_batch_v1(const ccfj_batch_args* args, void* stream) {
+  ccfj::clear_error();
+  int st = ccfj::batch_validate(args);
+  if (st != CCFJ_OK) return st;
+  if (!args->device_ptrs) return ccfj::batch_host(*args, (cudaStream_t)stream);
+  CCFJ_REQUIRE(args->total_pairs >= args->nsets,
+               "ccfj_fj_batch_v1: device mode needs total_pairs (= offsets[nsets])");
+  return ccfj::batch_run_device(*args, args->total_pairs, (cudaStream_t)stream);
+}
+
+CCFJ_API int ccfj_batch_graph_cache_clear(void) {
+  std::lock_guard<std::mutex> lk(ccfj::g_graph_mu);
+  for (auto& kv : ccfj::g_graphs)
+    if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+  ccfj::g_graphs.clear();
+  return CCFJ_OK;
+}

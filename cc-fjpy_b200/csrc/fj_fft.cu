@@ -110,8 +110,8 @@ __global__ void __launch_bounds__(kFftThreads) rfft_pow2_kernel(FftJob job, cons
 // Direct DFT for lengths that are not powers of two: one thread per
 // (row, bin); the phase index k n mod N is exact in 64-bit integers.
 __global__ void rdft_kernel(FftJob job) {
-  const int kk = blockIdx.x * blockDim.x + threadIdx.x;
-  const int row = blockIdx.y;
+  const int kk = blockIdx.y * blockDim.x + threadIdx.x;
+  const int row = blockIdx.x;
   if (kk >= job.nbins) return;
   const long long k = (long long)kk * job.bin_stride;
   float2* out = job.out + (long long)row * job.nbins;
@@ -163,7 +163,7 @@ int rfft_bins(const FftJob& job, int nrows_out, cudaStream_t s, Scratch& sc) {
     count_launch();
     CCFJ_LAUNCH_CHECK("rfft_pow2_kernel");
   } else {
-    rdft_kernel<<<dim3(div_up(job.nbins, 128), nrows_out), 128, 0, s>>>(job);
+    rdft_kernel<<<dim3(nrows_out, div_up(job.nbins, 128)), 128, 0, s>>>(job);
     count_launch();
     CCFJ_LAUNCH_CHECK("rdft_kernel");
   }

@@ -98,6 +98,52 @@ typedef struct ccfj_fj_args {
 
 CCFJ_API int ccfj_fj_v1(const ccfj_fj_args *args, void *stream);
 
+/* -------------------------------------------------------- ragged batch
+ * Many data sets (subarrays) with their own pairs, distances and spectra
+ * but shared f and c grids, in one persistent launch: equivalent to calling
+ * the transform once per set (fj_noise per subarray), with the sets' pairs
+ * concatenated. Set b owns pairs offsets[b] .. offsets[b+1]-1 (each set
+ * non-empty, distances ascending within it); perm maps pair i to its row of
+ * u (global rows). out is [nsets][nc][nf]. FP32 only.
+ *   use_graph = 1: the launch sequence is captured once per distinct
+ *     argument set into a CUDA graph and replayed on later calls (device
+ *     mode; ignored when the stream is already being captured by the
+ *     caller, or when a caller allocator is installed).
+ *   variant: velocities per thread, 1, 2 or 4 (0 = 2).
+ * No counterpart in the reference, which has no batch entry.
+ */
+typedef struct ccfj_batch_args {
+  int struct_size;     /* sizeof(ccfj_batch_args)                              */
+  int nsets;           /* data sets                                            */
+  int nf, nc;          /* shared frequency / velocity grids                    */
+  int itype, mode;     /* as ccfj_fj_args                                      */
+  int precision;       /* CCFJ_PREC_FP32 only                                  */
+  int normalize;       /* per (set, frequency) max-abs normalisation           */
+  int device_ptrs;     /* as ccfj_fj_args                                      */
+  int hilbert;         /* as ccfj_fj_args (mode J_MINUS_Y, u[1] = NULL)        */
+  int use_graph;       /* capture and replay a CUDA graph (device mode)        */
+  int variant;         /* 0, 1, 2 or 4                                         */
+  const long long *offsets; /* [nsets + 1], offsets[0] = 0                     */
+  long long total_pairs;    /* offsets[nsets] (required in device mode)        */
+  const float *r;      /* [total_pairs], ascending within each set             */
+  const float *u[2];   /* spectra rows, layout as ccfj_fj_args                 */
+  long long u_ld;
+  long long u_rows;
+  int u_es;
+  int u_ncols;
+  int fstride;
+  const long long *perm; /* optional [total_pairs]                            */
+  const float *f;
+  const float *c;
+  float *out;          /* [nsets][nc][nf]                                      */
+  float tau;
+} ccfj_batch_args;
+
+CCFJ_API int ccfj_fj_batch_v1(const ccfj_batch_args *args, void *stream);
+/* Destroys the cached batch graphs (call before freeing buffers that a
+ * cached graph refers to, if their addresses may be reused). */
+CCFJ_API int ccfj_batch_graph_cache_clear(void);
+
 /* ------------------------------------------ allocation-free transform
  * No counterpart in the reference. The same FP32 transform as ccfj_fj_v1
  * with device pointers (device_ptrs = 1, precision CCFJ_PREC_FP32,
