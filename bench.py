@@ -448,6 +448,8 @@ def run_config(args):
         else:
             rng = np.random.default_rng(4)
             ntr, npts, Fs, nf, nwin = 1000, 16384, 10.0, 1024, 64
+            if getattr(args, "mwfj_small", False):
+                nf, nwin = 256, 8
             r = np.exp(rng.uniform(np.log(5e3), np.log(1.5e6), ntr))
             c = np.linspace(1500, 5000, 2000)
         u = cases.ricker_records(rng, r, npts, Fs)
@@ -574,13 +576,19 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
-    ap.add_argument("--profile-case", action="store_true",
-                    help="run only the device transform on a 512-frequency slice of the workload "
-                         "(steps launches, no extras): the case the ncu captures use")
+    ap.add_argument("--profile-case", nargs="?", const="noise", default=None,
+                    choices=("noise", "mwfj"),
+                    help="run only the device transform on a reduced case (steps launches, no "
+                         "extras) for ncu captures: 'noise' = the first 512 frequencies of the "
+                         "workload; 'mwfj' = the MWFJ configuration with 8 windows and 256 bins")
     ap.add_argument("--config", type=int, default=0, choices=(0, 1, 3, 4, 5),
                     help="time another SURVEY configuration (device-resident; one JSON line)")
     args = ap.parse_args()
     if args.config:
+        return run_config(args)
+    if args.profile_case == "mwfj":
+        args.config = 4
+        args.mwfj_small = True
         return run_config(args)
     if args.profile_case:
         return run_profile_case(args)

@@ -464,6 +464,14 @@ int batch_host(const ccfj_batch_args& a, cudaStream_t s) {
 
 }  // namespace
 
+int normalize_sets(float* out, int nsets, int nc, int nf, cudaStream_t s) {
+  CCFJ_REQUIRE(nsets <= 65535, "normalisation of %d sets (> 65535)", nsets);
+  batch_normalize_kernel<<<dim3(div_up(nf, 32), nsets), dim3(32, 8), 0, s>>>(out, nc, nf);
+  count_launch();
+  CCFJ_LAUNCH_CHECK("batch_normalize_kernel");
+  return CCFJ_OK;
+}
+
 }  // namespace ccfj
 
 CCFJ_API int ccfj_fj_batch_v1(const ccfj_batch_args* args, void* stream) {

@@ -331,4 +331,9 @@ __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
   }
 }
 
+// Launches fj_prep_geom_kernel (drs, trapezoid weights of sorted r).
+void fj_prep_geom_kernel_shared(const float* rs, int nr, float* drs, float* wtr, cudaStream_t s);
+// Per (set, frequency) column normalisation of out[nsets][nc][nf].
+int normalize_sets(float* out, int nsets, int nc, int nf, cudaStream_t s);
+
 }  // namespace ccfj

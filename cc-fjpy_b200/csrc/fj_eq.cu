@@ -84,6 +84,10 @@ static int eq_device(const ccfj_eq_args& a, cudaStream_t s) {
   int st = rfft_bins(job, (int)rows_out, s, sc);
   if (st != CCFJ_OK) return st;
 
+  // MWFJ: all windows share the pairs, so their transforms share the
+  // interval moments (one pass over the geometry for a tile of windows).
+  if (a.nwin > 0 && a.precision == CCFJ_PREC_FP32) return mwfj_cuda_core(a, spec, s, sc);
+
   // One transform per window over its [ntr][nf] complex spectra: input 0 is
   // the real part, input 1 the imaginary part (element stride 2).
   for (int w = 0; w < nw; ++w) {

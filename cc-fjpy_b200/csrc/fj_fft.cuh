@@ -28,4 +28,8 @@ struct FftJob {
 // Runs the front end for nrows_out rows (row = w * ntr + i).
 int rfft_bins(const FftJob& job, int nrows_out, cudaStream_t s, Scratch& sc);
 
+// MWFJ transform of all windows at once from their spectra
+// ([nwin][ntr][nf] complex, sorted traces), CUDA-core contraction.
+int mwfj_cuda_core(const ccfj_eq_args& a, const float2* spec, cudaStream_t s, Scratch& sc);
+
 }  // namespace ccfj

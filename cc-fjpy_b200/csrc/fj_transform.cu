@@ -123,6 +123,10 @@ __global__ void __launch_bounds__(256) fj_plain64_kernel(FjDev a, const float* g
   a.out[(long long)ci * a.nf + fi] = finish<MODE, double>(acc, 1.0);
 }
 
+void fj_prep_geom_kernel_shared(const float* rs, int nr, float* drs, float* wtr, cudaStream_t s) {
+  fj_prep_geom_kernel<<<div_up(nr, 256), 256, 0, s>>>(rs, nr, drs, wtr);
+}
+
 // Gathered plain copy of one input, [nr][nf] float (for the comparator).
 __global__ void fj_gather_kernel(InDesc in, int nr, int nf, float* __restrict__ dst) {
   const int fi = blockIdx.y * blockDim.x + threadIdx.x;

@@ -163,3 +163,28 @@ def test_invalid_func_and_shape(ccfj, capsys):
     eq = cases.eq_case("eq_small")
     with pytest.raises(ValueError, match="cannot reshape"):
         ccfj.fj_earthquake(eq["u"], eq["r"], eq["c"], eq["f"], fstride=2)
+
+
+@pytest.mark.parametrize("itype", [0, 1])
+@pytest.mark.parametrize("func", [0, 1])
+def test_mwfj_window_tiles(ccfj, itype, func):
+    """10 windows: one full tile of 8 windows and a partial tile of 2 share
+    each station evaluation; every window matches the FP64 oracle and the
+    single-window transform of the windowed traces."""
+    rng = np.random.default_rng(41)
+    npts, Fs, ntr, nwin = 256, 10.0, 14, 10
+    r = np.exp(rng.uniform(np.log(5e3), np.log(1.5e5), ntr))
+    u = cases.ricker_records(rng, r, npts, Fs)
+    L = rng.integers(40, 200, size=(nwin, ntr))
+    start = rng.integers(0, npts - L)
+    winl, winr = start / Fs, (start + L) / Fs
+    f = Fs * np.arange(24) / npts
+    c = np.linspace(1500, 5000, 33)
+    y = _quiet(ccfj.MWFJ, u, r, c, f, Fs, nwin, winl, winr, taper=0.9, itype=itype, func=func)
+    y64 = O.MWFJ(u, r, c, f, Fs, nwin, winl, winr, taper=0.9, itype=itype, func=func,
+                 normalize=False)
+    for w in range(nwin):
+        assert O.rel_error(y[w], O._normalize(y64[w])) <= TOL
+        uw = np.stack([u[j] * ccfj.win(npts, Fs, winl[w, j], winr[w, j], 0.9) for j in range(ntr)])
+        single = _quiet(ccfj.fj_earthquake, uw, r, c, f, itype=itype, func=func)
+        assert O.rel_error(y[w], single) <= TOL
