@@ -42,6 +42,8 @@ class EqArgs(ctypes.Structure):
 
 _lib.SIGNATURES["ccfj_fj_earthquake_v1"] = (ctypes.c_int, [ctypes.POINTER(EqArgs),
                                                             ctypes.c_void_p])
+_lib.SIGNATURES["ccfj_set_mwfj_path"] = (ctypes.c_int, [ctypes.c_int])
+_lib.SIGNATURES["ccfj_device_status"] = (ctypes.c_int, [ctypes.c_void_p])
 
 
 def _check_bins(nr, npts, nf, fstride):

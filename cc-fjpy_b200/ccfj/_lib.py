@@ -94,8 +94,10 @@ def load():
     global _LIB
     if _LIB is not None:
         return _LIB
-    path = _build.LIB
+    path = os.environ.get("CCFJ_LIB_PATH") or _build.LIB
     if not os.path.exists(path):
+        if path != _build.LIB:
+            raise FileNotFoundError("CCFJ_LIB_PATH=%s does not exist" % path)
         _build.build()
     lib = ctypes.CDLL(path)
     for name, (res, args) in SIGNATURES.items():

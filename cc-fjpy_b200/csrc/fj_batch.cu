@@ -44,6 +44,7 @@ __global__ void batch_prep_geom_kernel(const float* __restrict__ rs,
                                        long long total, float* __restrict__ drs,
                                        float* __restrict__ wtr) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == total) drs[total] = 0.0f;  // padding read by the one-station lookahead
   if (i >= total) return;
   const int b = set_of(off, nsets, i);
   const long long s = off[b], e = off[b + 1];
@@ -260,7 +261,7 @@ int batch_validate(const ccfj_batch_args* a) {
 int batch_device(const ccfj_batch_args& a, long long total, cudaStream_t s) {
   Scratch sc(s);
   const int nin = nin_of_mode(a.mode);
-  float* drs = sc.get_n<float>(total);
+  float* drs = sc.get_n<float>(total + 1);
   float* wtr = sc.get_n<float>(total);
   int* order = sc.get_n<int>(a.nsets);
   unsigned long long* counter = sc.get_n<unsigned long long>(1);
@@ -272,7 +273,7 @@ int batch_device(const ccfj_batch_args& a, long long total, cudaStream_t s) {
     batch_identity_order_kernel<<<div_up(a.nsets, 256), 256, 0, s>>>(a.nsets, order);
   count_launch();
   CCFJ_LAUNCH_CHECK("batch_order_kernel");
-  batch_prep_geom_kernel<<<div_up(total, 256), 256, 0, s>>>(a.r, a.offsets, a.nsets, total, drs,
+  batch_prep_geom_kernel<<<div_up(total + 1, 256), 256, 0, s>>>(a.r, a.offsets, a.nsets, total, drs,
                                                              wtr);
   count_launch();
   CCFJ_LAUNCH_CHECK("batch_prep_geom_kernel");
@@ -310,7 +311,7 @@ int batch_device(const ccfj_batch_args& a, long long total, cudaStream_t s) {
   bd.off = a.offsets;
   bd.order = order;
   bd.nsets = a.nsets;
-  const int cpt = a.variant > 0 ? a.variant : 2;
+  const int cpt = a.variant > 0 ? a.variant : default_cpt_for(a.mode, a.itype);
   bd.ftiles = div_up(a.nf, 32);
   bd.ctiles = div_up(a.nc, 8 * cpt);
   bd.items = (long long)a.nsets * bd.ftiles * bd.ctiles;

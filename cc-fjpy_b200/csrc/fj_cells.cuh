@@ -105,7 +105,7 @@ struct Cell<double> {
 
 struct FjDev {
   const float* rs;
-  const float* drs;
+  const float* drs;  // [nr + 1]: r_i - r_{i-1}, 0 at i = 0 and at i = nr
   const void* gb[2];
   const float* f;
   const float* c;
@@ -149,31 +149,28 @@ __global__ void fj_prep_u_kernel(InDesc in, int nr, int nf, const float* __restr
 }
 
 // ------------------------------------------------- station-amortised kernel
+// acc += g_{i-1} I0 + b_i I1 / k per input and basis (I1k = I1 / k); the
+// sum is formed with one FMA per term.
 template <int MODE, typename T>
 __device__ __forceinline__ void accumulate_interval(T (&acc)[2], const typename Vec2<T>::type& g0,
-                                                    const typename Vec2<T>::type& g1, T scale_b,
-                                                    T I0J, T I1J, T I0Y, T I1Y) {
-  const T b0 = g0.y * scale_b;
+                                                    const typename Vec2<T>::type& g1, T I0J,
+                                                    T I1Jk, T I0Y, T I1Yk) {
+  using fjs::fmaT;
   if (MODE == CCFJ_MODE_J) {
-    acc[0] += fjs::fmaT(g0.x, I0J, b0 * I1J);
+    acc[0] = fmaT(g0.y, I1Jk, fmaT(g0.x, I0J, acc[0]));
   } else if (MODE == CCFJ_MODE_Y) {
-    acc[0] += fjs::fmaT(g0.x, I0Y, b0 * I1Y);
-  } else {
-    const T b1 = g1.y * scale_b;
-    const T J0 = fjs::fmaT(g0.x, I0J, b0 * I1J);  // J basis on input 0
-    const T J1 = fjs::fmaT(g1.x, I0J, b1 * I1J);  // J basis on input 1
-    if (MODE == CCFJ_MODE_J_MINUS_Y) {
-      const T Y1 = fjs::fmaT(g1.x, I0Y, b1 * I1Y);
-      acc[0] += J0 - Y1;
-    } else if (MODE == CCFJ_MODE_ABS_J) {
-      acc[0] += J0;
-      acc[1] += J1;
-    } else {  // ABS_H: (J(u0) - Y(u1)) + i (J(u1) + Y(u0))
-      const T Y0 = fjs::fmaT(g0.x, I0Y, b0 * I1Y);
-      const T Y1 = fjs::fmaT(g1.x, I0Y, b1 * I1Y);
-      acc[0] += J0 - Y1;
-      acc[1] += J1 + Y0;
-    }
+    acc[0] = fmaT(g0.y, I1Yk, fmaT(g0.x, I0Y, acc[0]));
+  } else if (MODE == CCFJ_MODE_J_MINUS_Y) {
+    acc[0] = fmaT(g0.y, I1Jk, fmaT(g0.x, I0J, acc[0]));
+    acc[0] = fmaT(-g1.y, I1Yk, fmaT(-g1.x, I0Y, acc[0]));
+  } else if (MODE == CCFJ_MODE_ABS_J) {
+    acc[0] = fmaT(g0.y, I1Jk, fmaT(g0.x, I0J, acc[0]));
+    acc[1] = fmaT(g1.y, I1Jk, fmaT(g1.x, I0J, acc[1]));
+  } else {  // ABS_H: (J(u0) - Y(u1)) + i (J(u1) + Y(u0))
+    acc[0] = fmaT(g0.y, I1Jk, fmaT(g0.x, I0J, acc[0]));
+    acc[0] = fmaT(-g1.y, I1Yk, fmaT(-g1.x, I0Y, acc[0]));
+    acc[1] = fmaT(g1.y, I1Jk, fmaT(g1.x, I0J, acc[1]));
+    acc[1] = fmaT(g0.y, I1Yk, fmaT(g0.x, I0Y, acc[1]));
   }
 }
 
@@ -234,7 +231,7 @@ __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
     Station<T> sJp[CPT], sYp[CPT];
     T xp[CPT];
     T r_cur = (T)__ldg(a.rs);
-    T dr_next = a.nr > 1 ? (T)__ldg(a.drs + 1) : T(0);
+    T dr_next = (T)__ldg(a.drs + 1);  // drs has nr + 1 entries, the last 0
 #pragma unroll
     for (int j = 0; j < CPT; ++j) {
       xp[j] = cell[j].k * r_cur;
@@ -260,7 +257,7 @@ __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
       for (int i = i0; i < i1; ++i) {
         const T r = (T)__ldg(a.rs + i);
         const T dr = dr_next;
-        dr_next = i + 1 < a.nr ? (T)__ldg(a.drs + i + 1) : T(0);
+        dr_next = (T)__ldg(a.drs + i + 1);
         using T2 = typename Vec2<T>::type;
         const long long gidx = (long long)i * a.nf + fi;
         const T2 g0 = __ldg(static_cast<const T2*>(a.gb[0]) + gidx);
@@ -288,7 +285,8 @@ __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
             fjs::interval_moments<T>(sYp[j], sY, dx, lcY, I0Y, I1Y);
             sYp[j] = sY;
           }
-          accumulate_interval<MODE, T>(acc[j], g0, g1, cell[j].inv_k, I0J, I1J, I0Y, I1Y);
+          accumulate_interval<MODE, T>(acc[j], g0, g1, I0J, I1J * cell[j].inv_k, I0Y,
+                                       I1Y * cell[j].inv_k);
           xp[j] = x;
         }
       }
@@ -331,8 +329,11 @@ __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
   }
 }
 
-// Launches fj_prep_geom_kernel (drs, trapezoid weights of sorted r).
+// Launches fj_prep_geom_kernel: drs [nr + 1] (drs[0] = drs[nr] = 0) and the
+// trapezoid weights wtr [nr] of the sorted r.
 void fj_prep_geom_kernel_shared(const float* rs, int nr, float* drs, float* wtr, cudaStream_t s);
+// Default velocities per thread of the FP32 kernel for a mode and itype.
+int default_cpt_for(int mode, int itype);
 // Per (set, frequency) column normalisation of out[nsets][nc][nf].
 int normalize_sets(float* out, int nsets, int nc, int nf, cudaStream_t s);
 

@@ -86,7 +86,13 @@ static int eq_device(const ccfj_eq_args& a, cudaStream_t s) {
 
   // MWFJ: all windows share the pairs, so their transforms share the
   // interval moments (one pass over the geometry for a tile of windows).
-  if (a.nwin > 0 && a.precision == CCFJ_PREC_FP32) return mwfj_cuda_core(a, spec, s, sc);
+  if (a.nwin > 0 && a.precision == CCFJ_PREC_FP32) {
+    // tensor cores when the window dimension makes the contraction dense
+    const bool tc_ok = a.itype == 1 && a.func == 0 && a.ntr >= 2 && a.nwin <= 128;
+    const bool use_tc = tc_ok && (g_mwfj_path == 2 || (g_mwfj_path == 0 && a.nwin >= 8));
+    if (use_tc) return mwfj_tensor(a, spec, s, sc);
+    return mwfj_cuda_core(a, spec, s, sc);
+  }
 
   // One transform per window over its [ntr][nf] complex spectra: input 0 is
   // the real part, input 1 the imaginary part (element stride 2).
@@ -169,10 +175,33 @@ static int eq_host(const ccfj_eq_args& a, cudaStream_t s) {
   CCFJ_CUDA_TRY(cudaMemcpyAsync(a.out, dout, sizeof(float) * nw * a.nc * a.nf,
                                 cudaMemcpyDeviceToHost, s));
   CCFJ_CUDA_TRY(cudaStreamSynchronize(s));
+  bool failed = false;
+  st = mw_tc_error(s, &failed);
+  if (st != CCFJ_OK) return st;
+  if (failed)
+    return set_error(CCFJ_ERR_TIMEOUT, "ccfj_fj_earthquake_v1: a bounded device wait ran out");
   return CCFJ_OK;
 }
 
+int g_mwfj_path = 0;
+
 }  // namespace ccfj
+
+CCFJ_API int ccfj_set_mwfj_path(int path) {
+  if (path < 0 || path > 2)
+    return ccfj::set_error(CCFJ_ERR_INVALID, "ccfj_set_mwfj_path: path must be 0, 1 or 2");
+  ccfj::g_mwfj_path = path;
+  return CCFJ_OK;
+}
+
+CCFJ_API int ccfj_device_status(void* stream) {
+  ccfj::clear_error();
+  bool failed = false;
+  const int st = ccfj::mw_tc_error((cudaStream_t)stream, &failed);
+  if (st != CCFJ_OK) return st;
+  if (failed) return ccfj::set_error(CCFJ_ERR_TIMEOUT, "a bounded device wait ran out");
+  return CCFJ_OK;
+}
 
 CCFJ_API int ccfj_fj_earthquake_v1(const ccfj_eq_args* args, void* stream) {
   ccfj::clear_error();

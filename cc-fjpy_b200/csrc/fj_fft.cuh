@@ -31,5 +31,12 @@ int rfft_bins(const FftJob& job, int nrows_out, cudaStream_t s, Scratch& sc);
 // MWFJ transform of all windows at once from their spectra
 // ([nwin][ntr][nf] complex, sorted traces), CUDA-core contraction.
 int mwfj_cuda_core(const ccfj_eq_args& a, const float2* spec, cudaStream_t s, Scratch& sc);
+// The same contraction on the tensor cores (tcgen05, BF16x3): itype 1,
+// func 0, 2 <= nr, nwin <= 128.
+int mwfj_tensor(const ccfj_eq_args& a, const float2* spec, cudaStream_t s, Scratch& sc);
+// Reads (and waits for) the tensor kernel's timeout flag.
+int mw_tc_error(cudaStream_t s, bool* failed);
+// 0 = automatic, 1 = CUDA cores, 2 = tensor cores where supported.
+extern int g_mwfj_path;
 
 }  // namespace ccfj

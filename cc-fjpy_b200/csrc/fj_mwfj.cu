@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(256) fj_mw_kernel(MwDev a) {
     const float tau = a.tau;
     Station<float> sJp, sYp;
     float xp = cell.k * __ldg(a.rs);
-    float dr_next = a.nr > 1 ? __ldg(a.drs + 1) : 0.f;
+    float dr_next = __ldg(a.drs + 1);  // drs has nr + 1 entries, the last 0
     cell.eval<WJ, WY, true>(__ldg(a.rs), xp, closed_form<float, WY>(cell.k * dr_next, xp, tau),
                             Jz, Yz);
     sJp = fjs::make_station(xp, Jz);
@@ -112,7 +112,7 @@ __global__ void __launch_bounds__(256) fj_mw_kernel(MwDev a) {
       for (int i = i0; i < i1; ++i) {
         const float r = __ldg(a.rs + i);
         const float dr = dr_next;
-        dr_next = i + 1 < a.nr ? __ldg(a.drs + i + 1) : 0.f;
+        dr_next = __ldg(a.drs + i + 1);
         const float x = cell.k * r;
         const float dx = cell.k * dr;
         const bool lcJ = lnJ, lcY = lnY;
@@ -216,7 +216,7 @@ void launch_mw(const MwDev& d, int nwt, cudaStream_t s) {
 // distances `rs` sorted. Writes out [nwin][nc][nf] (normalised if asked).
 int mwfj_cuda_core(const ccfj_eq_args& a, const float2* spec, cudaStream_t s, Scratch& sc) {
   const int nr = a.ntr, nf = a.nf, nwin = a.nwin;
-  float* drs = sc.get_n<float>(nr);
+  float* drs = sc.get_n<float>(nr + 1);
   float* wtr = sc.get_n<float>(nr);
   if (!drs || !wtr) return CCFJ_ERR_ALLOC;
   fj_prep_geom_kernel_shared(a.r, nr, drs, wtr, s);

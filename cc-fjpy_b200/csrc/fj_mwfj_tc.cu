@@ -1,0 +1,480 @@
+// MWFJ contraction on the 5th-generation tensor cores (tcgen05, sm_100a).
+//
+// For one frequency f the multi-window transform is a matrix product
+//
+//   D[c, n] = sum_k A[c, k] B[k, n]
+//     A[c, (i, 0)] = I0_i(f, c)          A[c, (i, 1)] = I1_i(f, c) / k
+//     B[(i, 0), n] = g_{i-1, n}(f)       B[(i, 1), n] = b_{i, n}(f)
+//
+// over the intervals i of the shared pair geometry, with n = 2 w + part the
+// real / imaginary part of window w, followed by |D[c, 2w] + i D[c, 2w+1]| /
+// k^2 (fj_earthquake's magnitude, src/ccfj-gpu.pyx:282-284) and the
+// per-frequency normalisation. A is generated on the fly (the station-
+// amortised FP32 special functions, one thread per velocity); B is the
+// windows' interval data, prepared once. Both are split into bf16 hi + lo
+// parts and the product is formed as A_hi B_hi + A_hi B_lo + A_lo B_hi
+// with FP32 accumulation in tensor memory (BF16x3, about 16 bits of
+// mantissa per operand).
+//
+// CTA: 256 threads = 256 velocities (two M = 128 accumulators), one
+// frequency, all windows (N = 2 nwin padded to a multiple of 16, <= 256).
+// Per chunk of 16 intervals (K = 32): every thread writes its 32 A values
+// (hi and lo) into shared memory in the K-major, no-swizzle canonical
+// layout; one thread waits for the chunk's B (a 1-D bulk copy, issued two
+// chunks ahead), issues 12 tcgen05.mma and commits them to an mbarrier that
+// releases the stage. Two stages. All waits are bounded; a wait that runs
+// out sets an error flag, drains what is in flight and returns.
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#include "fj_cells.cuh"
+#include "fj_fft.cuh"
+
+namespace ccfj {
+
+namespace tc {
+
+constexpr int kThreads = 256;       // velocities per CTA (2 x M = 128)
+constexpr int kChunkI = 16;         // intervals per chunk
+constexpr int kChunkK = 2 * kChunkI;  // K per chunk (I0 and I1/k per interval)
+constexpr int kSlices = kChunkK / 16;  // MMA K = 16 for bf16
+constexpr int kSliceBytes128 = 128 * 16 * 2;  // one K-slice of a 128-row operand: 4096 B
+constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 2 GHz: a wait longer than this is an error
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait: false if the phase did not complete within kWaitCycles.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity)) {
+    if (clock64() - t0 > kWaitCycles) return false;
+  }
+  return true;
+}
+
+// 1-D bulk copy global -> shared, completion counted on `bar` (no multicast).
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void fence_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+// K-major, no-swizzle shared-memory matrix descriptor: core matrices of 8
+// rows x 16 bytes, LBO = bytes between the two K halves of an MMA K-slice,
+// SBO = bytes between 8-row groups; version 1 (tcgen05).
+__device__ __forceinline__ uint64_t smem_desc(const void* p, uint32_t lbo, uint32_t sbo) {
+  const uint32_t a = smem_u32(p);
+  uint64_t d = 0;
+  d |= (uint64_t)((a >> 4) & 0x3FFF);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+  d |= (uint64_t)1 << 46;  // version
+  return d;                // base offset 0, legacy LBO mode, SWIZZLE_NONE
+}
+
+// Instruction descriptor of kind::f16: BF16 A and B (K-major), F32 D.
+__host__ __device__ constexpr uint32_t instr_desc_bf16(int M, int N) {
+  return (1u << 4)                       // D format F32
+         | (1u << 7)                     // A format BF16
+         | (1u << 10)                    // B format BF16
+         | ((uint32_t)(N >> 3) << 17)    // N / 8
+         | ((uint32_t)(M >> 4) << 24);   // M / 16
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc,
+                                         uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+          smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+      "%12, %13, %14, %15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+// bf16 hi / lo split of v: hi = rn(v), lo = rn(v - hi).
+__device__ __forceinline__ void split_bf16(float v, __nv_bfloat16& hi, __nv_bfloat16& lo) {
+  hi = __float2bfloat16_rn(v);
+  lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+}
+
+}  // namespace tc
+
+struct MwTcDev {
+  const float* rs;
+  const float* drs;         // [nr + 1]
+  const uint4* bchunks;     // [nf][nchunks] chunks of (hi, lo) B tiles, chunk_bytes each
+  const float* f;
+  const float* c;
+  float* out;               // [nwin][nc][nf]
+  unsigned int* err;        // set to 1 when a bounded wait runs out
+  int nr, nf, nc, nwin;
+  int N;                    // 2 nwin padded to a multiple of 16
+  int nchunks;              // ceil((nr - 1) / kChunkI)
+  int tmem_cols;            // power of two >= 2 N
+  float tau;
+};
+
+// Shared-memory layout of one CTA (dynamic):
+//   A[stage][half m][hi/lo][slice] 128 rows x 16 K bf16   2*2*2*2*4096 = 64 KB
+//   B[stage][hi/lo][slice]         N rows x 16 K bf16     2*2*2*(N*32) B
+//   barriers, tmem address
+struct TcSmem {
+  static constexpr int kABytesStage = 2 * 2 * tc::kSlices * tc::kSliceBytes128;
+  __host__ __device__ static int b_bytes_stage(int N) { return 2 * tc::kSlices * N * 32; }
+  __host__ __device__ static int total(int N) {
+    return 2 * kABytesStage + 2 * b_bytes_stage(N) + 64;
+  }
+};
+
+// Byte offset of element (row, k) inside one 128-row (or N-row) operand
+// tile of kSlices K-slices: slice = k / 16, half = (k % 16) / 8.
+__device__ __forceinline__ int tile_off(int row, int k, int rows) {
+  const int slice = k >> 4, kk = k & 15;
+  return slice * rows * 32 + (row >> 3) * 256 + (kk >> 3) * 128 + (row & 7) * 16 + (kk & 7) * 2;
+}
+
+__global__ void __launch_bounds__(tc::kThreads, 2) fj_mw_tc_kernel(MwTcDev a) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  const int tid = threadIdx.x;
+  const int fi = blockIdx.y;
+  const int c0 = blockIdx.x * tc::kThreads;
+  const int ci = min(c0 + tid, a.nc - 1);
+  unsigned char* sA = smem;
+  unsigned char* sB = smem + 2 * TcSmem::kABytesStage;
+  const int bstage = TcSmem::b_bytes_stage(a.N);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sB + 2 * bstage);  // [0,1] B full, [2,3] MMA done
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 4);
+  __shared__ int abort_flag;
+
+  if (tid == 0) {
+    for (int j = 0; j < 4; ++j) tc::mbar_init(bar + j, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    abort_flag = 0;
+  }
+  if (tid < 32) {  // warp 0 owns the tensor-memory allocation
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     tc::smem_u32(tmem_slot)),
+                 "r"(a.tmem_cols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t tmem = *tmem_slot;
+
+  const uint4* bsrc = a.bchunks + (long long)fi * a.nchunks * (bstage / 16);
+  // issue B for chunks 0 and 1
+  if (tid == 0) {
+    for (int kc = 0; kc < 2 && kc < a.nchunks; ++kc) {
+      tc::mbar_expect_tx(bar + kc, bstage);
+      tc::bulk_g2s(sB + kc * bstage, bsrc + (long long)kc * (bstage / 16), bstage, bar + kc);
+    }
+  }
+
+  // per-thread generator state (one velocity)
+  Cell<float> cell;
+  cell.init(a.f[fi], a.c[ci]);
+  const float tau = a.tau;
+  ZB<float> Jz{};
+  ZB<float> Yz{};
+  Station<float> sp;
+  float xp = cell.k * __ldg(a.rs);
+  float dr_next = __ldg(a.drs + 1);
+  cell.eval<true, false, true>(__ldg(a.rs), xp, closed_form<float, false>(cell.k * dr_next, xp, tau),
+                               Jz, Yz);
+  sp = fjs::make_station(xp, Jz);
+  bool ln = closed_form<float, false>(cell.k * dr_next, xp, tau);
+
+  const int mh = tid >> 7;      // accumulator (M half)
+  const int row = tid & 127;    // row inside it
+  const uint32_t idesc = tc::instr_desc_bf16(128, a.N);
+  int issued_b = a.nchunks < 2 ? a.nchunks : 2;  // B copies issued (thread 0's count)
+  int committed = 0;                             // MMA groups committed (thread 0's count)
+
+  // Every abort decision is taken on abort_flag right after a barrier, so
+  // all threads leave the loop together.
+  for (int kc = 0; kc < a.nchunks; ++kc) {
+    const int s = kc & 1;
+    if (kc >= 2) {
+      // the MMAs of chunk kc - 2 released this stage
+      if (!tc::mbar_wait(bar + 2 + s, ((kc >> 1) - 1) & 1)) atomicOr(&abort_flag, 1);
+      __syncthreads();
+      if (abort_flag) break;
+      if (tid == 0) {
+        tc::mbar_expect_tx(bar + s, bstage);
+        tc::bulk_g2s(sB + s * bstage, bsrc + (long long)kc * (bstage / 16), bstage, bar + s);
+        ++issued_b;
+      }
+    }
+    // A of this chunk: I0 and I1/k of intervals 1 + 16 kc + j
+    unsigned char* aHi = sA + s * TcSmem::kABytesStage + mh * (2 * tc::kSlices * tc::kSliceBytes128);
+    unsigned char* aLo = aHi + tc::kSlices * tc::kSliceBytes128;
+#pragma unroll 1
+    for (int j4 = 0; j4 < tc::kChunkI; j4 += 4) {
+      __nv_bfloat16 hi[8], lo[8];
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj) {
+        const int i = 1 + kc * tc::kChunkI + j4 + jj;
+        float I0 = 0.f, I1k = 0.f;
+        if (i < a.nr) {
+          const float r = __ldg(a.rs + i);
+          const float dr = dr_next;
+          dr_next = __ldg(a.drs + i + 1);
+          const float x = cell.k * r;
+          const float dx = cell.k * dr;
+          const bool lc = ln;
+          ln = closed_form<float, false>(cell.k * dr_next, x, tau);
+          cell.eval<true, false, true>(r, x, lc || ln, Jz, Yz);
+          const Station<float> st = fjs::make_station(x, Jz);
+          float I1;
+          fjs::interval_moments<float>(sp, st, dx, lc, I0, I1);
+          sp = st;
+          xp = x;
+          I1k = I1 * cell.inv_k;
+        }
+        tc::split_bf16(I0, hi[2 * jj], lo[2 * jj]);
+        tc::split_bf16(I1k, hi[2 * jj + 1], lo[2 * jj + 1]);
+      }
+      const int off = tile_off(row, 2 * j4, 128);
+      *reinterpret_cast<uint4*>(aHi + off) = *reinterpret_cast<const uint4*>(hi);
+      *reinterpret_cast<uint4*>(aLo + off) = *reinterpret_cast<const uint4*>(lo);
+    }
+    tc::fence_async_smem();
+    tc::tc_fence_before();
+    __syncthreads();
+    if (tid == 0) {
+      tc::tc_fence_after();
+      if (!tc::mbar_wait(bar + s, (kc >> 1) & 1)) {
+        atomicOr(&abort_flag, 1);
+      } else {
+        unsigned char* bHi = sB + s * bstage;
+        unsigned char* bLo = bHi + tc::kSlices * a.N * 32;
+        for (int m = 0; m < 2; ++m) {
+          unsigned char* ah = sA + s * TcSmem::kABytesStage + m * (2 * tc::kSlices * tc::kSliceBytes128);
+          unsigned char* al = ah + tc::kSlices * tc::kSliceBytes128;
+          const uint32_t d = tmem + (uint32_t)(m * a.N);  // accumulator m: columns [m N, (m+1) N)
+          for (int sl = 0; sl < tc::kSlices; ++sl) {
+            const uint64_t dah = tc::smem_desc(ah + sl * tc::kSliceBytes128, 128, 256);
+            const uint64_t dal = tc::smem_desc(al + sl * tc::kSliceBytes128, 128, 256);
+            const uint64_t dbh = tc::smem_desc(bHi + sl * a.N * 32, 128, 256);
+            const uint64_t dbl = tc::smem_desc(bLo + sl * a.N * 32, 128, 256);
+            const uint32_t acc0 = (kc > 0 || sl > 0) ? 1u : 0u;
+            tc::mma_bf16(d, dah, dbh, idesc, acc0);
+            tc::mma_bf16(d, dah, dbl, idesc, 1u);
+            tc::mma_bf16(d, dal, dbh, idesc, 1u);
+          }
+        }
+        tc::mma_commit(bar + 2 + s);
+        ++committed;
+      }
+    }
+    __syncthreads();
+    if (abort_flag) break;
+  }
+
+  // Drain: wait for the last committed MMA group (its commit covers every
+  // earlier MMA of this thread) and, after an abort, for every B copy still
+  // in flight, before reading or freeing anything.
+  __shared__ int n_committed, n_issued, drain_fail;
+  if (tid == 0) {
+    n_committed = committed;
+    n_issued = issued_b;
+    drain_fail = 0;
+  }
+  __syncthreads();
+  if (n_committed > 0) {
+    const int last = n_committed - 1;
+    if (!tc::mbar_wait(bar + 2 + (last & 1), (last >> 1) & 1)) atomicOr(&drain_fail, 1);
+  }
+  if (abort_flag && tid == 0) {
+    for (int kc = n_committed; kc < n_issued; ++kc)
+      if (!tc::mbar_wait(bar + (kc & 1), (kc >> 1) & 1)) atomicOr(&drain_fail, 1);
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  tc::tc_fence_after();
+  if (!abort_flag && !drain_fail && n_committed == a.nchunks) {
+    // epilogue: row `row` of accumulator `mh` -> |Re + i Im| / k^2
+    const uint32_t tbase = tmem + ((uint32_t)(tid & 96) << 16) + (uint32_t)(mh * a.N);
+    const int c = c0 + tid;
+    for (int col = 0; col < a.N; col += 16) {
+      float v[16];
+      tc::tmem_ld16(tbase + (uint32_t)col, v);
+      if (c < a.nc) {
+#pragma unroll
+        for (int j = 0; j < 16; j += 2) {
+          const int w = (col + j) >> 1;
+          if (w < a.nwin) {
+            const float re = v[j] * cell.inv_k2, im = v[j + 1] * cell.inv_k2;
+            a.out[((long long)w * a.nc + c) * a.nf + fi] = sqrtf(re * re + im * im);
+          }
+        }
+      }
+    }
+  } else if (tid == 0) {
+    atomicOr(a.err, 1u);
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  if (tid < 32) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(a.tmem_cols));
+  }
+}
+
+// B chunks from the windows' spectra spec[w][i][f] (complex): chunk (f, kc)
+// holds, for n = 2 w + part and K index (j, p) of interval i = 1 + 16 kc + j,
+// p = 0: g_{i-1}, p = 1: (g_i - g_{i-1}) / max(dr_i, 0.1), split into bf16
+// hi (first half of the chunk) and lo, in the K-major canonical layout.
+__global__ void mw_tc_prep_kernel(const float2* __restrict__ spec, int ntr, int nf, int nwin, int N,
+                                  int nchunks, const float* __restrict__ drs,
+                                  unsigned char* __restrict__ dst) {
+  const int fi = blockIdx.y * blockDim.x + threadIdx.x;  // frequency fastest: coalesced reads
+  const int n = blockIdx.z;                               // B row (window part)
+  const int i = 1 + blockIdx.x;                           // interval, 1 .. nchunks*16
+  if (fi >= nf) return;
+  const int w = n >> 1, part = n & 1;
+  float g0 = 0.f, b = 0.f;
+  if (w < nwin && i < ntr) {
+    const float2 cur = spec[((long long)w * ntr + i) * nf + fi];
+    const float2 prv = spec[((long long)w * ntr + i - 1) * nf + fi];
+    const float gc = part ? cur.y : cur.x, gp = part ? prv.y : prv.x;
+    g0 = gp;
+    b = (gc - gp) / fmaxf(drs[i], 0.1f);
+  }
+  const int kc = (i - 1) / tc::kChunkI, j = (i - 1) % tc::kChunkI;
+  const long long chunk_bytes = 2LL * tc::kSlices * N * 32;
+  unsigned char* base = dst + ((long long)fi * nchunks + kc) * chunk_bytes;
+  const int off = tile_off(n, 2 * j, N);
+  __nv_bfloat16 h0, l0, h1, l1;
+  tc::split_bf16(g0, h0, l0);
+  tc::split_bf16(b, h1, l1);
+  __nv_bfloat162 hh, ll;
+  hh.x = h0;
+  hh.y = h1;
+  ll.x = l0;
+  ll.y = l1;
+  *reinterpret_cast<__nv_bfloat162*>(base + off) = hh;
+  *reinterpret_cast<__nv_bfloat162*>(base + tc::kSlices * N * 32 + off) = ll;
+}
+
+// Device flag written by the tensor-core kernel when a bounded wait ran out.
+__device__ unsigned int g_mw_tc_error = 0;
+
+int mwfj_tensor(const ccfj_eq_args& a, const float2* spec, cudaStream_t s, Scratch& sc) {
+  const int nr = a.ntr, nf = a.nf, nwin = a.nwin;
+  CCFJ_REQUIRE(nr >= 2 && nwin >= 1, "MWFJ tensor path: needs nr >= 2 and nwin >= 1");
+  int N = 2 * nwin;
+  N = (N + 15) / 16 * 16;
+  CCFJ_REQUIRE(N <= 256, "MWFJ tensor path: at most 128 windows (got %d)", nwin);
+  int cols = 32;
+  while (cols < 2 * N) cols <<= 1;
+  float* drs = sc.get_n<float>(nr + 1);
+  float* wtr = sc.get_n<float>(nr);
+  if (!drs || !wtr) return CCFJ_ERR_ALLOC;
+  fj_prep_geom_kernel_shared(a.r, nr, drs, wtr, s);
+  count_launch();
+  CCFJ_LAUNCH_CHECK("fj_prep_geom_kernel");
+  const int nchunks = (nr - 1 + tc::kChunkI - 1) / tc::kChunkI;
+  const long long chunk_bytes = 2LL * tc::kSlices * N * 32;
+  unsigned char* bch = static_cast<unsigned char*>(sc.get((size_t)nf * nchunks * chunk_bytes));
+  if (!bch) return CCFJ_ERR_ALLOC;
+  mw_tc_prep_kernel<<<dim3(nchunks * tc::kChunkI, div_up(nf, 32), N), 32, 0, s>>>(
+      spec, nr, nf, nwin, N, nchunks, drs, bch);
+  count_launch();
+  CCFJ_LAUNCH_CHECK("mw_tc_prep_kernel");
+  unsigned int* err = nullptr;
+  CCFJ_CUDA_TRY(cudaGetSymbolAddress((void**)&err, g_mw_tc_error));
+  CCFJ_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(unsigned int), s));
+  MwTcDev d{};
+  d.rs = a.r;
+  d.drs = drs;
+  d.bchunks = reinterpret_cast<const uint4*>(bch);
+  d.f = a.f;
+  d.c = a.c;
+  d.out = a.out;
+  d.err = err;
+  d.nr = nr;
+  d.nf = nf;
+  d.nc = a.nc;
+  d.nwin = nwin;
+  d.N = N;
+  d.nchunks = nchunks;
+  d.tmem_cols = cols;
+  d.tau = a.tau > 0 ? a.tau : kDefaultTau32;
+  const int smem = TcSmem::total(N);
+  CCFJ_CUDA_TRY(cudaFuncSetAttribute(fj_mw_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  prof_begin(s);
+  fj_mw_tc_kernel<<<dim3(div_up(a.nc, tc::kThreads), nf), tc::kThreads, smem, s>>>(d);
+  prof_end(s);
+  count_launch();
+  CCFJ_LAUNCH_CHECK("fj_mw_tc_kernel");
+  if (a.normalize) return normalize_sets(a.out, nwin, a.nc, nf, s);
+  return CCFJ_OK;
+}
+
+int mw_tc_error(cudaStream_t s, bool* failed) {
+  unsigned int h = 0;
+  CCFJ_CUDA_TRY(cudaMemcpyFromSymbolAsync(&h, g_mw_tc_error, sizeof(h), 0, cudaMemcpyDeviceToHost, s));
+  CCFJ_CUDA_TRY(cudaStreamSynchronize(s));
+  *failed = h != 0;
+  return CCFJ_OK;
+}
+
+}  // namespace ccfj

@@ -39,6 +39,7 @@ using fjs::ZB;
 __global__ void fj_prep_geom_kernel(const float* __restrict__ rs, int nr, float* __restrict__ drs,
                                     float* __restrict__ wtr) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i == nr) drs[nr] = 0.0f;  // padding read by the kernels' one-station lookahead
   if (i >= nr) return;
   const float r = rs[i];
   const float dl = i > 0 ? r - rs[i - 1] : 0.0f;
@@ -50,8 +51,11 @@ __global__ void fj_prep_geom_kernel(const float* __restrict__ rs, int nr, float*
   wtr[i] = (w0 + w1) * 0.5f * r;
 }
 
+#ifndef CCFJ_FJ_MIN_BLOCKS
+#define CCFJ_FJ_MIN_BLOCKS 1
+#endif
 template <int MODE, int ITYPE, typename T, int CPT>
-__global__ void __launch_bounds__(256) fj_amortized_kernel(FjDev a) {
+__global__ void __launch_bounds__(256, CCFJ_FJ_MIN_BLOCKS) fj_amortized_kernel(FjDev a) {
   fj_cells<MODE, ITYPE, T, CPT>(a, blockIdx.x * blockDim.x + threadIdx.x,
                                 (blockIdx.y * blockDim.y + threadIdx.y) * CPT);
 }
@@ -124,7 +128,7 @@ __global__ void __launch_bounds__(256) fj_plain64_kernel(FjDev a, const float* g
 }
 
 void fj_prep_geom_kernel_shared(const float* rs, int nr, float* drs, float* wtr, cudaStream_t s) {
-  fj_prep_geom_kernel<<<div_up(nr, 256), 256, 0, s>>>(rs, nr, drs, wtr);
+  fj_prep_geom_kernel<<<div_up(nr + 1, 256), 256, 0, s>>>(rs, nr, drs, wtr);
 }
 
 // Gathered plain copy of one input, [nr][nf] float (for the comparator).
@@ -238,10 +242,24 @@ long long tune_key(const ccfj_fj_args& a) {
 }
 }  // namespace
 
+// Untuned default per mode (measured on the large-array workload): two
+// velocities per thread for one basis and one input, four for the
+// two-input Bessel form and the trapezoid, one for the two-basis forms
+// (their register use leaves too few warps resident with more).
+int default_cpt_for(int mode, int itype) {
+  if (itype == 0) return 4;
+  switch (mode) {
+    case CCFJ_MODE_J:
+    case CCFJ_MODE_Y: return 2;
+    case CCFJ_MODE_ABS_J: return 4;
+    default: return 1;
+  }
+}
+
 int tuned_cpt(const ccfj_fj_args& a) {
   std::lock_guard<std::mutex> lk(g_tune_mu);
   auto it = g_tune.find(tune_key(a));
-  return it == g_tune.end() ? 2 : it->second;
+  return it == g_tune.end() ? default_cpt_for(a.mode, a.itype) : it->second;
 }
 
 void record_tuned_cpt(const ccfj_fj_args& a, int cpt) {
@@ -253,10 +271,10 @@ void record_tuned_cpt(const ccfj_fj_args& a, int cpt) {
 int fj_device(const ccfj_fj_args& a, cudaStream_t s) {
   const int nin = nin_of(a.mode);
   Scratch sc(s);
-  float* drs = sc.get_n<float>(a.nr);
+  float* drs = sc.get_n<float>(a.nr + 1);
   float* wtr = sc.get_n<float>(a.nr);
   if (!drs || !wtr) return CCFJ_ERR_ALLOC;
-  fj_prep_geom_kernel<<<div_up(a.nr, 256), 256, 0, s>>>(a.r, a.nr, drs, wtr);
+  fj_prep_geom_kernel<<<div_up(a.nr + 1, 256), 256, 0, s>>>(a.r, a.nr, drs, wtr);
   count_launch();
   CCFJ_LAUNCH_CHECK("fj_prep_geom_kernel");
 
@@ -658,7 +676,7 @@ static int fj_noalloc(const ccfj_fj_args& a, cudaStream_t s) {
                      "ccfj_fj_noalloc_v1: hilbert = 1 is not supported; pass the transformed "
                      "spectrum as u[1]");
   const int nin = nin_of(a.mode);
-  const size_t geom = round256(sizeof(float) * (size_t)a.nr);
+  const size_t geom = round256(sizeof(float) * ((size_t)a.nr + 1));
   const size_t per_input = round256((size_t)a.nr * a.nf * (a.itype == 1 ? 8 : 4));
   const size_t need = 2 * geom + nin * per_input;
   if (need > kNoAllocScratchBytes)
@@ -676,7 +694,7 @@ static int fj_noalloc(const ccfj_fj_args& a, cudaStream_t s) {
   // kernels of this call, so nothing needs clearing between calls.
   float* drs = reinterpret_cast<float*>(p);
   float* wtr = reinterpret_cast<float*>(p + geom);
-  fj_prep_geom_kernel<<<div_up(a.nr, 256), 256, 0, s>>>(a.r, a.nr, drs, wtr);
+  fj_prep_geom_kernel<<<div_up(a.nr + 1, 256), 256, 0, s>>>(a.r, a.nr, drs, wtr);
   count_launch();
   CCFJ_LAUNCH_CHECK("fj_prep_geom_kernel");
 

@@ -109,7 +109,8 @@ CCFJ_API int ccfj_fj_v1(const ccfj_fj_args *args, void *stream);
  *     argument set into a CUDA graph and replayed on later calls (device
  *     mode; ignored when the stream is already being captured by the
  *     caller, or when a caller allocator is installed).
- *   variant: velocities per thread, 1, 2 or 4 (0 = 2).
+ *   variant: velocities per thread, 1, 2 or 4 (0 = the per-mode default of
+ *     ccfj_set_fj_variant).
  * No counterpart in the reference, which has no batch entry.
  */
 typedef struct ccfj_batch_args {
@@ -204,6 +205,15 @@ typedef struct ccfj_eq_args {
 } ccfj_eq_args;
 
 CCFJ_API int ccfj_fj_earthquake_v1(const ccfj_eq_args *args, void *stream);
+/* MWFJ contraction of the windows: 0 = automatic (tensor cores, tcgen05
+ * BF16x3 with FP32 accumulation, for itype 1, func 0 and 8 <= nwin <= 128;
+ * CUDA-core FMAs otherwise), 1 = always CUDA cores, 2 = tensor cores
+ * wherever supported. */
+CCFJ_API int ccfj_set_mwfj_path(int path);
+/* Waits for `stream` and reports CCFJ_ERR_TIMEOUT if a bounded device-side
+ * wait of a tensor-core kernel ran out since the last such launch (host-
+ * memory calls check this themselves). */
+CCFJ_API int ccfj_device_status(void *stream);
 
 /* ------------------------------------------------------------- tuning
  * The FP32 kernels come in variants that give each thread 1, 2 or 4
@@ -211,7 +221,8 @@ CCFJ_API int ccfj_fj_earthquake_v1(const ccfj_eq_args *args, void *stream);
  * (device pointers; out is overwritten), records the fastest for the
  * problem's class (mode, itype and the powers of two of nr, nf, nc) for all
  * later calls of this process, and returns it. ccfj_set_fj_variant(cpt)
- * forces a variant (0 restores the tuned/default choice, which is 2). */
+ * forces a variant (0 restores the tuned choice, or the per-mode default:
+ * 2 for MODE_J / MODE_Y, 4 for MODE_ABS_J and for itype 0, 1 otherwise). */
 CCFJ_API int ccfj_autotune_fj_v1(const ccfj_fj_args *args, void *stream, int *best_cpt,
                                  float *best_ms);
 CCFJ_API int ccfj_set_fj_variant(int cpt);
