@@ -29,6 +29,33 @@ void clear_error() { g_last_error.clear(); }
 
 void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
+// Scratch comes from one stream-ordered memory pool per device that keeps
+// its memory between calls (release threshold = max): without it, every
+// call would map its multi-GB scratch afresh from the driver.
+static cudaMemPool_t library_pool() {
+  static std::mutex mu;
+  static cudaMemPool_t pools[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> lk(mu);
+  if (!pools[dev]) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t p = nullptr;
+    if (cudaMemPoolCreate(&p, &props) != cudaSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    uint64_t keep = ~0ull;
+    cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+    pools[dev] = p;
+  }
+  return pools[dev];
+}
+
 void* dev_alloc(size_t bytes, cudaStream_t s) {
   if (bytes == 0) bytes = 256;
   ccfj_alloc_fn fn;
@@ -44,7 +71,12 @@ void* dev_alloc(size_t bytes, cudaStream_t s) {
     return p;
   }
   void* p = nullptr;
-  cudaError_t e = cudaMallocAsync(&p, bytes, s);
+  // during stream capture the allocation becomes a graph memory node, which
+  // the graph manages itself: take it from the default pool then
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (s) cudaStreamIsCapturing(s, &cs);
+  cudaMemPool_t pool = cs == cudaStreamCaptureStatusNone ? library_pool() : nullptr;
+  cudaError_t e = pool ? cudaMallocFromPoolAsync(&p, bytes, pool, s) : cudaMallocAsync(&p, bytes, s);
   if (e != cudaSuccess) {
     cudaGetLastError();
     set_error(CCFJ_ERR_ALLOC, "cudaMallocAsync(%zu) failed: %s", bytes, cudaGetErrorString(e));

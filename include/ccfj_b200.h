@@ -247,9 +247,10 @@ CCFJ_API double ccfj_profile_total_ms(int *count);
  * transform kernels, which are bound by the FP32 pipe. */
 CCFJ_API int ccfj_fp32_peak_probe(void *stream, double *tflops);
 
-/* Replaces the device allocator (NULL, NULL restores the default
- * stream-ordered cudaMallocAsync/cudaFreeAsync). alloc returns NULL on
- * failure; both receive the cudaStream_t of the call as void*. */
+/* Replaces the device allocator of the library's scratch memory (NULL, NULL
+ * restores the default: stream-ordered allocation from a library-owned
+ * memory pool per device that keeps its memory between calls). alloc returns
+ * NULL on failure; both receive the cudaStream_t of the call as void*. */
 typedef void *(*ccfj_alloc_fn)(size_t bytes, void *stream, void *user);
 typedef void (*ccfj_free_fn)(void *ptr, void *stream, void *user);
 CCFJ_API int ccfj_set_allocator(ccfj_alloc_fn alloc, ccfj_free_fn free_fn, void *user);
