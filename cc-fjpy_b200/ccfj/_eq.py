@@ -44,6 +44,7 @@ _lib.SIGNATURES["ccfj_fj_earthquake_v1"] = (ctypes.c_int, [ctypes.POINTER(EqArgs
                                                             ctypes.c_void_p])
 _lib.SIGNATURES["ccfj_set_mwfj_path"] = (ctypes.c_int, [ctypes.c_int])
 _lib.SIGNATURES["ccfj_device_status"] = (ctypes.c_int, [ctypes.c_void_p])
+_lib.SIGNATURES["ccfj_self_test_wait_timeout"] = (ctypes.c_int, [ctypes.c_void_p])
 
 
 def _check_bins(nr, npts, nf, fstride):

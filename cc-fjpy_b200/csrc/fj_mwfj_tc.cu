@@ -67,11 +67,11 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait: false if the phase did not complete within kWaitCycles.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// Bounded wait: false if the phase did not complete within `limit` cycles.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, long long limit) {
   const long long t0 = clock64();
   while (!mbar_try_wait(bar, parity)) {
-    if (clock64() - t0 > kWaitCycles) return false;
+    if (clock64() - t0 > limit) return false;
   }
   return true;
 }
@@ -168,6 +168,8 @@ struct MwTcDev {
   int nchunks;              // ceil((nr - 1) / kChunkI)
   int tmem_cols;            // power of two >= 2 N
   float tau;
+  long long wait_cycles;    // limit of every mbarrier wait (tc::kWaitCycles)
+  int self_test_no_copy;    // self-test only: issue no B copy, so the first wait runs out
 };
 
 // Shared-memory layout of one CTA (dynamic):
@@ -220,7 +222,7 @@ __global__ void __launch_bounds__(tc::kThreads, 2) fj_mw_tc_kernel(MwTcDev a) {
 
   const uint4* bsrc = a.bchunks + (long long)fi * a.nchunks * (bstage / 16);
   // issue B for chunks 0 and 1
-  if (tid == 0) {
+  if (tid == 0 && !a.self_test_no_copy) {
     for (int kc = 0; kc < 2 && kc < a.nchunks; ++kc) {
       tc::mbar_expect_tx(bar + kc, bstage);
       tc::bulk_g2s(sB + kc * bstage, bsrc + (long long)kc * (bstage / 16), bstage, bar + kc);
@@ -244,7 +246,7 @@ __global__ void __launch_bounds__(tc::kThreads, 2) fj_mw_tc_kernel(MwTcDev a) {
   const int mh = tid >> 7;      // accumulator (M half)
   const int row = tid & 127;    // row inside it
   const uint32_t idesc = tc::instr_desc_bf16(128, a.N);
-  int issued_b = a.nchunks < 2 ? a.nchunks : 2;  // B copies issued (thread 0's count)
+  int issued_b = a.self_test_no_copy ? 0 : (a.nchunks < 2 ? a.nchunks : 2);  // thread 0's count
   int committed = 0;                             // MMA groups committed (thread 0's count)
 
   // Every abort decision is taken on abort_flag right after a barrier, so
@@ -253,10 +255,10 @@ __global__ void __launch_bounds__(tc::kThreads, 2) fj_mw_tc_kernel(MwTcDev a) {
     const int s = kc & 1;
     if (kc >= 2) {
       // the MMAs of chunk kc - 2 released this stage
-      if (!tc::mbar_wait(bar + 2 + s, ((kc >> 1) - 1) & 1)) atomicOr(&abort_flag, 1);
+      if (!tc::mbar_wait(bar + 2 + s, ((kc >> 1) - 1) & 1, a.wait_cycles)) atomicOr(&abort_flag, 1);
       __syncthreads();
       if (abort_flag) break;
-      if (tid == 0) {
+      if (tid == 0 && !a.self_test_no_copy) {
         tc::mbar_expect_tx(bar + s, bstage);
         tc::bulk_g2s(sB + s * bstage, bsrc + (long long)kc * (bstage / 16), bstage, bar + s);
         ++issued_b;
@@ -300,7 +302,7 @@ __global__ void __launch_bounds__(tc::kThreads, 2) fj_mw_tc_kernel(MwTcDev a) {
     __syncthreads();
     if (tid == 0) {
       tc::tc_fence_after();
-      if (!tc::mbar_wait(bar + s, (kc >> 1) & 1)) {
+      if (!tc::mbar_wait(bar + s, (kc >> 1) & 1, a.wait_cycles)) {
         atomicOr(&abort_flag, 1);
       } else {
         unsigned char* bHi = sB + s * bstage;
@@ -340,11 +342,11 @@ __global__ void __launch_bounds__(tc::kThreads, 2) fj_mw_tc_kernel(MwTcDev a) {
   __syncthreads();
   if (n_committed > 0) {
     const int last = n_committed - 1;
-    if (!tc::mbar_wait(bar + 2 + (last & 1), (last >> 1) & 1)) atomicOr(&drain_fail, 1);
+    if (!tc::mbar_wait(bar + 2 + (last & 1), (last >> 1) & 1, a.wait_cycles)) atomicOr(&drain_fail, 1);
   }
   if (abort_flag && tid == 0) {
     for (int kc = n_committed; kc < n_issued; ++kc)
-      if (!tc::mbar_wait(bar + (kc & 1), (kc >> 1) & 1)) atomicOr(&drain_fail, 1);
+      if (!tc::mbar_wait(bar + (kc & 1), (kc >> 1) & 1, a.wait_cycles)) atomicOr(&drain_fail, 1);
   }
   tc::tc_fence_before();
   __syncthreads();
@@ -417,6 +419,8 @@ __global__ void mw_tc_prep_kernel(const float2* __restrict__ spec, int ntr, int 
 // Device flag written by the tensor-core kernel when a bounded wait ran out.
 __device__ unsigned int g_mw_tc_error = 0;
 
+int mw_tc_error(cudaStream_t s, bool* failed);
+
 int mwfj_tensor(const ccfj_eq_args& a, const float2* spec, cudaStream_t s, Scratch& sc) {
   const int nr = a.ntr, nf = a.nf, nwin = a.nwin;
   CCFJ_REQUIRE(nr >= 2 && nwin >= 1, "MWFJ tensor path: needs nr >= 2 and nwin >= 1");
@@ -458,6 +462,8 @@ int mwfj_tensor(const ccfj_eq_args& a, const float2* spec, cudaStream_t s, Scrat
   d.nchunks = nchunks;
   d.tmem_cols = cols;
   d.tau = a.tau > 0 ? a.tau : kDefaultTau32;
+  d.wait_cycles = tc::kWaitCycles;
+  d.self_test_no_copy = 0;
   const int smem = TcSmem::total(N);
   CCFJ_CUDA_TRY(cudaFuncSetAttribute(fj_mw_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   prof_begin(s);
@@ -466,6 +472,61 @@ int mwfj_tensor(const ccfj_eq_args& a, const float2* spec, cudaStream_t s, Scrat
   count_launch();
   CCFJ_LAUNCH_CHECK("fj_mw_tc_kernel");
   if (a.normalize) return normalize_sets(a.out, nwin, a.nc, nf, s);
+  return CCFJ_OK;
+}
+
+// Self-test of the timeout path: one CTA of the tensor kernel on a tiny
+// problem whose B copy is never issued, with a ~1 ms wait limit. The kernel
+// must give up, set the error flag, free its tensor memory and return.
+int mw_tc_self_test(cudaStream_t s, int* status) {
+  Scratch sc(s);
+  const int N = 16, nr = 3, cols = 32;
+  const float host_r[3] = {1000.f, 2000.f, 3500.f};
+  const float host_fc[2] = {0.1f, 1000.f};
+  float* r = sc.get_n<float>(nr);
+  float* drs = sc.get_n<float>(nr + 1);
+  float* fc = sc.get_n<float>(2);
+  float* out = sc.get_n<float>(N);
+  unsigned char* bch = static_cast<unsigned char*>(sc.get(2 * tc::kSlices * N * 32));
+  if (!r || !drs || !fc || !out || !bch) return CCFJ_ERR_ALLOC;
+  CCFJ_CUDA_TRY(cudaMemcpyAsync(r, host_r, sizeof(host_r), cudaMemcpyHostToDevice, s));
+  CCFJ_CUDA_TRY(cudaMemcpyAsync(fc, host_fc, sizeof(host_fc), cudaMemcpyHostToDevice, s));
+  CCFJ_CUDA_TRY(cudaMemsetAsync(bch, 0, 2 * tc::kSlices * N * 32, s));
+  float* wtr = sc.get_n<float>(nr);
+  if (!wtr) return CCFJ_ERR_ALLOC;
+  fj_prep_geom_kernel_shared(r, nr, drs, wtr, s);
+  unsigned int* err = nullptr;
+  CCFJ_CUDA_TRY(cudaGetSymbolAddress((void**)&err, g_mw_tc_error));
+  CCFJ_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(unsigned int), s));
+  MwTcDev d{};
+  d.rs = r;
+  d.drs = drs;
+  d.bchunks = reinterpret_cast<const uint4*>(bch);
+  d.f = fc;
+  d.c = fc + 1;
+  d.out = out;
+  d.err = err;
+  d.nr = nr;
+  d.nf = 1;
+  d.nc = 1;
+  d.nwin = 1;
+  d.N = N;
+  d.nchunks = 1;
+  d.tmem_cols = cols;
+  d.tau = kDefaultTau32;
+  d.wait_cycles = 2000000;  // ~1 ms
+  d.self_test_no_copy = 1;
+  const int smem = TcSmem::total(N);
+  CCFJ_CUDA_TRY(cudaFuncSetAttribute(fj_mw_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  fj_mw_tc_kernel<<<1, tc::kThreads, smem, s>>>(d);
+  count_launch();
+  CCFJ_LAUNCH_CHECK("fj_mw_tc_kernel (self-test)");
+  bool failed = false;
+  const int st = mw_tc_error(s, &failed);
+  if (st != CCFJ_OK) return st;
+  *status = failed ? CCFJ_ERR_TIMEOUT : CCFJ_OK;
+  CCFJ_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(unsigned int), s));
+  CCFJ_CUDA_TRY(cudaStreamSynchronize(s));
   return CCFJ_OK;
 }
 
@@ -478,3 +539,13 @@ int mw_tc_error(cudaStream_t s, bool* failed) {
 }
 
 }  // namespace ccfj
+
+CCFJ_API int ccfj_self_test_wait_timeout(void* stream) {
+  ccfj::clear_error();
+  int status = CCFJ_OK;
+  const int st = ccfj::mw_tc_self_test((cudaStream_t)stream, &status);
+  if (st != CCFJ_OK) return st;
+  if (status != CCFJ_ERR_TIMEOUT)
+    return ccfj::set_error(CCFJ_ERR_CUDA, "self-test: the tensor kernel did not report its timeout");
+  return CCFJ_OK;
+}

@@ -214,6 +214,11 @@ CCFJ_API int ccfj_set_mwfj_path(int path);
  * wait of a tensor-core kernel ran out since the last such launch (host-
  * memory calls check this themselves). */
 CCFJ_API int ccfj_device_status(void *stream);
+/* Self-test of the bounded waits: runs one CTA of the tensor-core MWFJ
+ * kernel whose input copy is never issued, with a ~1 ms wait limit, and
+ * returns CCFJ_OK if the kernel gave up, reported the timeout and left the
+ * device usable (CCFJ_ERR_CUDA otherwise). No counterpart in the reference. */
+CCFJ_API int ccfj_self_test_wait_timeout(void *stream);
 
 /* ------------------------------------------------------------- tuning
  * The FP32 kernels come in variants that give each thread 1, 2 or 4
