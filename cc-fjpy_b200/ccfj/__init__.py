@@ -62,12 +62,14 @@ def _float_rows(uf):
 
 
 def _transform(ufs, r, c, f, fstride, itype, mode, perm=None, hilbert=False, normalize=False,
-               precision=_lib.PREC_FP32):
+               precision=_lib.PREC_FP32, cols=None):
     """Runs ccfj_fj_v1 on host arrays. `ufs` holds one or two 2-D spectra
     of the same shape whose rows are pairs; `r` is in pair order (sorted by
-    the caller when perm is given: r[i] belongs to row perm[i])."""
+    the caller when perm is given: r[i] belongs to row perm[i]). `cols` =
+    (a, b) computes only frequencies a .. b-1 of f (f, out cover those)."""
     lib = _lib.load()
     nr, nc, nf = len(r), len(c), len(f)
+    a_col, b_col = (0, nf) if cols is None else cols
     u0 = np.asarray(ufs[0])
     if u0.ndim != 2:
         raise IndexError("too many indices for array: array is %d-dimensional, but 2 were indexed"
@@ -87,13 +89,14 @@ def _transform(ufs, r, c, f, fstride, itype, mode, perm=None, hilbert=False, nor
                 .reshape(nr, nf) for u in ufs]
         if perm is not None:
             flat = [x[perm] for x in flat]
-        return _transform(flat, r, c, f, 1, itype, mode, None, hilbert, normalize, precision)
+        return _transform(flat, r, c, f, 1, itype, mode, None, hilbert, normalize, precision, cols)
     bases = [_float_rows(u) for u in ufs]
-    r32, f32, c32 = _as_f32_vec(r), _as_f32_vec(f), _as_f32_vec(c)
-    out = np.empty((nc, nf), dtype=np.float32)
+    r32, f32, c32 = _as_f32_vec(r), _as_f32_vec(np.asarray(f)[a_col:b_col]), _as_f32_vec(c)
+    out = np.empty((nc, b_col - a_col), dtype=np.float32)
     a = _lib.FjArgs()
     a.struct_size = ctypes.sizeof(_lib.FjArgs)
-    a.nr, a.nf, a.nc = nr, nf, nc
+    a.nr, a.nf, a.nc = nr, b_col - a_col, nc
+    a.col_begin, a.nf_total = a_col, nf
     a.itype, a.mode, a.precision = int(itype), int(mode), int(precision)
     a.normalize = 1 if normalize else 0
     a.device_ptrs = 0
@@ -235,3 +238,4 @@ def CC(*args, **kwargs):
 
 from ._eq import fj_earthquake, MWFJ  # noqa: E402
 from ._batch import fj_noise_batch  # noqa: E402
+from . import dist  # noqa: E402,F401

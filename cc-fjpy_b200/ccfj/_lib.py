@@ -48,6 +48,8 @@ class FjArgs(ctypes.Structure):
         ("c", ctypes.c_void_p),
         ("out", ctypes.c_void_p),
         ("tau", ctypes.c_float),
+        ("col_begin", ctypes.c_int),
+        ("nf_total", ctypes.c_int),
     ]
 
 

@@ -285,7 +285,7 @@ int batch_device(const ccfj_batch_args& a, long long total, cudaStream_t s) {
     if (!hb) return CCFJ_ERR_ALLOC;
     CCFJ_REQUIRE(total <= INT_MAX, "ccfj_fj_batch_v1: too many pairs for the Hilbert transform");
     const int st = hilbert_rows(InDesc{a.u[0], a.u_ld, a.u_es, a.perm}, a.u_ncols, a.u_es,
-                                (int)total, a.nf, a.fstride, hb, s, sc);
+                                (int)total, a.nf, a.fstride, 0, hb, s, sc);
     if (st != CCFJ_OK) return st;
     in[1] = InDesc{hb, a.nf, 1, nullptr};
   }

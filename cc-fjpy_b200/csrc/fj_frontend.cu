@@ -41,7 +41,7 @@ constexpr int kHilMaxN = 16384;  // 3 n floats of shared memory (192 KiB)
 // tid sums outputs j = tid + 256 t: the x2 reads of a warp are consecutive
 // words (no bank conflicts) and the h read is a broadcast.
 __global__ void __launch_bounds__(kHilThreads) hilbert_rows_kernel(InDesc in, int n, int es, int nf,
-                                                                  int fstride,
+                                                                  int fstride, int col_begin,
                                                                   const float* __restrict__ h,
                                                                   float* __restrict__ dst) {
   extern __shared__ float sm[];
@@ -75,13 +75,14 @@ __global__ void __launch_bounds__(kHilThreads) hilbert_rows_kernel(InDesc in, in
 #pragma unroll
     for (int t = 0; t < kHilR; ++t) {
       const int j = j0 + threadIdx.x + t * kHilThreads;
-      if (j < n && j % fstride == 0) dst[(long long)i * nf + j / fstride] = acc[t];
+      const int col = j / fstride - col_begin;
+      if (j < n && j % fstride == 0 && col >= 0 && col < nf) dst[(long long)i * nf + col] = acc[t];
     }
   }
 }
 
-int hilbert_rows(const InDesc& in, int n, int es, int nr, int nf, int fstride, float* dst,
-                 cudaStream_t s, Scratch& sc) {
+int hilbert_rows(const InDesc& in, int n, int es, int nr, int nf, int fstride, int col_begin,
+                 float* dst, cudaStream_t s, Scratch& sc) {
   if (n > kHilMaxN)
     return set_error(CCFJ_ERR_UNSUPPORTED,
                      "Hilbert transform rows longer than %d columns are not supported (got %d)",
@@ -94,7 +95,7 @@ int hilbert_rows(const InDesc& in, int n, int es, int nr, int nf, int fstride, f
   const size_t smem = sizeof(float) * 3 * (size_t)n;
   CCFJ_CUDA_TRY(cudaFuncSetAttribute(hilbert_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)smem));
-  hilbert_rows_kernel<<<nr, kHilThreads, smem, s>>>(in, n, es, nf, fstride, h, dst);
+  hilbert_rows_kernel<<<nr, kHilThreads, smem, s>>>(in, n, es, nf, fstride, col_begin, h, dst);
   count_launch();
   CCFJ_LAUNCH_CHECK("hilbert_rows_kernel");
   return CCFJ_OK;

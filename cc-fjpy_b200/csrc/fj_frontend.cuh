@@ -15,9 +15,9 @@ struct InDesc {
 };
 
 // dst[i][fi] = (Hilbert transform along the full row of length n, element
-// stride es, of row(i))[fi * fstride]; dst is [nr][nf] float.
-int hilbert_rows(const InDesc& in, int n, int es, int nr, int nf, int fstride, float* dst,
-                 cudaStream_t s, Scratch& sc);
+// stride es, of row(i))[(col_begin + fi) * fstride]; dst is [nr][nf] float.
+int hilbert_rows(const InDesc& in, int n, int es, int nr, int nf, int fstride, int col_begin,
+                 float* dst, cudaStream_t s, Scratch& sc);
 
 // Device-resident transform (all pointers in args are device pointers).
 int fj_device(const ccfj_fj_args& a, cudaStream_t s);

@@ -290,13 +290,14 @@ int fj_device(const ccfj_fj_args& a, cudaStream_t s) {
   d.tau = a.tau > 0 ? a.tau : (a.precision == CCFJ_PREC_FP32 ? kDefaultTau32 : kDefaultTau64);
 
   InDesc in[2];
+  const long long col0 = (long long)a.col_begin * a.fstride * a.u_es;  // first computed column
   for (int j = 0; j < 2; ++j)
-    in[j] = InDesc{a.u[j], a.u_ld, (long long)a.u_es * a.fstride, a.perm};
+    in[j] = InDesc{a.u[j] ? a.u[j] + col0 : nullptr, a.u_ld, (long long)a.u_es * a.fstride, a.perm};
   if (a.hilbert) {
     float* hb = sc.get_n<float>((size_t)a.nr * a.nf);
     if (!hb) return CCFJ_ERR_ALLOC;
     const int st = hilbert_rows(InDesc{a.u[0], a.u_ld, a.u_es, a.perm}, a.u_ncols, a.u_es, a.nr,
-                                a.nf, a.fstride, hb, s, sc);
+                                a.nf, a.fstride, a.col_begin, hb, s, sc);
     if (st != CCFJ_OK) return st;
     in[1] = InDesc{hb, a.nf, 1, nullptr};
   }
@@ -372,9 +373,13 @@ static int validate(const ccfj_fj_args* a) {
   CCFJ_REQUIRE(a->r && a->f && a->c && a->out && a->u[0], "ccfj_fj_v1: NULL array");
   CCFJ_REQUIRE(a->fstride >= 1 && a->u_es >= 1 && a->u_ld >= 1,
                "ccfj_fj_v1: fstride, u_es and u_ld must be >= 1");
-  CCFJ_REQUIRE(a->u_ncols >= 1 && (a->u_ncols + a->fstride - 1) / a->fstride == a->nf,
-               "ccfj_fj_v1: %d columns with fstride %d give %d frequencies, not nf=%d", a->u_ncols,
-               a->fstride, (a->u_ncols + a->fstride - 1) / a->fstride, a->nf);
+  const int nf_total = a->nf_total > 0 ? a->nf_total : a->nf;
+  CCFJ_REQUIRE(a->u_ncols >= 1 && (a->u_ncols + a->fstride - 1) / a->fstride == nf_total,
+               "ccfj_fj_v1: %d columns with fstride %d give %d frequencies, not %d", a->u_ncols,
+               a->fstride, (a->u_ncols + a->fstride - 1) / a->fstride, nf_total);
+  CCFJ_REQUIRE(a->col_begin >= 0 && a->col_begin + a->nf <= nf_total,
+               "ccfj_fj_v1: frequencies %d..%d outside the %d the rows hold", a->col_begin,
+               a->col_begin + a->nf - 1, nf_total);
   CCFJ_REQUIRE(a->u_ld >= (long long)(a->u_ncols - 1) * a->u_es + 1,
                "ccfj_fj_v1: u_ld=%lld too small for %d columns of stride %d", a->u_ld, a->u_ncols,
                a->u_es);
@@ -711,7 +716,8 @@ static int fj_noalloc(const ccfj_fj_args& a, cudaStream_t s) {
   const dim3 pb(32, 8), pg(div_up(a.nr, 8), div_up(a.nf, 32));
   for (int j = 0; j < nin; ++j) {
     void* g = p + 2 * geom + j * per_input;
-    const InDesc in{a.u[j], a.u_ld, (long long)a.u_es * a.fstride, a.perm};
+    const InDesc in{a.u[j] + (long long)a.col_begin * a.fstride * a.u_es, a.u_ld,
+                    (long long)a.u_es * a.fstride, a.perm};
     fj_prep_u_kernel<float><<<pg, pb, 0, s>>>(in, a.nr, a.nf, drs, wtr, a.itype, g);
     count_launch();
     CCFJ_LAUNCH_CHECK("fj_prep_u_kernel");

@@ -94,6 +94,9 @@ typedef struct ccfj_fj_args {
   const float *c;      /* [nc]                                                  */
   float *out;          /* [nc, nf]                                              */
   float tau;           /* Hermite/closed-form switch in k*dr; <= 0: default    */
+  int col_begin;       /* compute frequencies col_begin .. col_begin + nf - 1  */
+  int nf_total;        /*    of the nf_total the rows hold (0: nf_total = nf); */
+                       /*    f and out hold the computed frequencies only     */
 } ccfj_fj_args;
 
 CCFJ_API int ccfj_fj_v1(const ccfj_fj_args *args, void *stream);

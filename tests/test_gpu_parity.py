@@ -188,3 +188,19 @@ def test_mwfj_window_tiles(ccfj, itype, func):
         uw = np.stack([u[j] * ccfj.win(npts, Fs, winl[w, j], winr[w, j], 0.9) for j in range(ntr)])
         single = _quiet(ccfj.fj_earthquake, uw, r, c, f, itype=itype, func=func)
         assert O.rel_error(y[w], single) <= TOL
+
+
+@pytest.mark.parametrize("func", [0, 1])
+@pytest.mark.parametrize("itype", [0, 1])
+def test_frequency_window_equals_full_transform(ccfj, func, itype):
+    """Computing frequencies a..b-1 only (the sharded path's unit) gives the
+    same bits as those columns of the full transform (the Hilbert transform
+    still runs along the full rows)."""
+    from ccfj import dist
+    case = cases.noise_case("noise_fstride2")
+    args = (case["uf"], case["r"], case["c"], case["f"], case["fstride"], itype, func)
+    full = _quiet(ccfj.fj_noise, *args[:4], fstride=case["fstride"], itype=itype, func=func)
+    nf = len(case["f"])
+    for a, b in ((0, 7), (7, 13), (13, nf), (3, 4)):
+        part = dist._cuda_columns(*args, (a, b))
+        assert np.array_equal(part, full[:, a:b], equal_nan=True)
