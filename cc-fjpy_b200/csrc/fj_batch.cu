@@ -42,7 +42,7 @@ __device__ __forceinline__ int set_of(const long long* __restrict__ off, int nse
 __global__ void batch_prep_geom_kernel(const float* __restrict__ rs,
                                        const long long* __restrict__ off, int nsets,
                                        long long total, float* __restrict__ drs,
-                                       float* __restrict__ wtr) {
+                                       float* __restrict__ wtr, float4* __restrict__ geo) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i == total) drs[total] = 0.0f;  // padding read by the one-station lookahead
   if (i >= total) return;
@@ -52,31 +52,34 @@ __global__ void batch_prep_geom_kernel(const float* __restrict__ rs,
   const float dl = i > s ? r - rs[i - 1] : 0.0f;
   const float dr = i + 1 < e ? rs[i + 1] - r : 0.0f;
   drs[i] = dl;
+  if (geo) geo[i] = station_geometry(r, dr);
   const float w0 = i > s ? fmaxf(dl, 0.1f) : 0.0f;
   const float w1 = i + 1 < e ? fmaxf(dr, 0.1f) : 0.0f;
   wtr[i] = (w0 + w1) * 0.5f * r;
 }
 
-// As fj_prep_u_kernel, with the interval data of each set's first pair zero.
+// As fj_prep_coef_kernel (itype 1) and fj_prep_u_kernel (itype 0), with
+// each set's first and last pair closing its interval chain.
 __global__ void batch_prep_u_kernel(InDesc in, const long long* __restrict__ off, int nsets,
-                                    long long total, int nf, const float* __restrict__ drs,
-                                    const float* __restrict__ wtr, int itype,
+                                    long long total, int nf, const float* __restrict__ rs,
+                                    const float* __restrict__ drs, const float* __restrict__ wtr,
+                                    const float4* __restrict__ geo,
+                                    const float* __restrict__ thr, int itype,
                                     void* __restrict__ dst) {
   // rows on grid x (up to 2^31 - 1 blocks), frequencies on grid y
   const int fi = blockIdx.y * blockDim.x + threadIdx.x;
   const long long i = (long long)blockIdx.x * blockDim.y + threadIdx.y;
   if (fi >= nf || i >= total) return;
-  const long long row = in.perm ? in.perm[i] : i;
-  const float g = in.p[row * in.ld + (long long)fi * in.cs];
+  const long long col = (long long)fi * in.cs;
+  const float g = in.p[(in.perm ? in.perm[i] : i) * in.ld + col];
   if (itype == 1) {
-    float2 v = make_float2(0.f, 0.f);
     const int b = set_of(off, nsets, i);
-    if (i > off[b]) {
-      const long long rowp = in.perm ? in.perm[i - 1] : i - 1;
-      const float gp = in.p[rowp * in.ld + (long long)fi * in.cs];
-      v = make_float2(gp, (g - gp) / fmaxf(drs[i], 0.1f));
-    }
-    static_cast<float2*>(dst)[i * nf + fi] = v;
+    const bool hl = i > off[b], hr = i + 1 < off[b + 1];
+    const float gl = hl ? in.p[(in.perm ? in.perm[i - 1] : i - 1) * in.ld + col] : 0.0f;
+    const float gr = hr ? in.p[(in.perm ? in.perm[i + 1] : i + 1) * in.ld + col] : 0.0f;
+    static_cast<StationCoef<float>*>(dst)[i * nf + fi] =
+        station_coef<float>(g, gl, gr, hl, hr, rs[i], hl ? rs[i - 1] : 0.0f, drs[i],
+                            hr ? drs[i + 1] : 0.0f, geo[i].w, thr[fi]);
   } else {
     static_cast<float*>(dst)[i * nf + fi] = g * wtr[i];
   }
@@ -134,9 +137,8 @@ struct BatchDev {
 };
 
 template <int MODE, int ITYPE, int CPT>
-__global__ void __launch_bounds__(256) fj_batch_persistent_kernel(BatchDev bd) {
+__global__ void __launch_bounds__(256, fj_min_blocks<float>()) fj_batch_persistent_kernel(BatchDev bd) {
   __shared__ long long item_s;
-  using T2 = float2;
   for (;;) {
     if (threadIdx.x == 0 && threadIdx.y == 0) item_s = (long long)atomicAdd(bd.counter, 1ULL);
     __syncthreads();
@@ -151,7 +153,8 @@ __global__ void __launch_bounds__(256) fj_batch_persistent_kernel(BatchDev bd) {
     a.nr = (int)(bd.off[b + 1] - o);
     a.rs += o;
     a.drs += o;
-    constexpr long long esz = ITYPE == 1 ? sizeof(T2) : sizeof(float);
+    if (ITYPE == 1) a.geo += o;
+    constexpr long long esz = ITYPE == 1 ? sizeof(StationCoef<float>) : sizeof(float);
     a.gb[0] = static_cast<const char*>(bd.base.gb[0]) + o * a.nf * esz;
     if (ModeTraits<MODE>::NIN > 1) a.gb[1] = static_cast<const char*>(bd.base.gb[1]) + o * a.nf * esz;
     a.out += (long long)b * a.nc * a.nf;
@@ -263,9 +266,10 @@ int batch_device(const ccfj_batch_args& a, long long total, cudaStream_t s) {
   const int nin = nin_of_mode(a.mode);
   float* drs = sc.get_n<float>(total + 1);
   float* wtr = sc.get_n<float>(total);
+  float4* geo = a.itype == 1 ? sc.get_n<float4>(total) : nullptr;
   int* order = sc.get_n<int>(a.nsets);
   unsigned long long* counter = sc.get_n<unsigned long long>(1);
-  if (!drs || !wtr || !order || !counter) return CCFJ_ERR_ALLOC;
+  if (!drs || !wtr || !order || !counter || (a.itype == 1 && !geo)) return CCFJ_ERR_ALLOC;
   CCFJ_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s));
   if (a.nsets <= kSortMax)
     batch_order_kernel<<<1, 1024, 0, s>>>(a.offsets, a.nsets, order);
@@ -274,7 +278,7 @@ int batch_device(const ccfj_batch_args& a, long long total, cudaStream_t s) {
   count_launch();
   CCFJ_LAUNCH_CHECK("batch_order_kernel");
   batch_prep_geom_kernel<<<div_up(total + 1, 256), 256, 0, s>>>(a.r, a.offsets, a.nsets, total, drs,
-                                                             wtr);
+                                                             wtr, geo);
   count_launch();
   CCFJ_LAUNCH_CHECK("batch_prep_geom_kernel");
 
@@ -290,16 +294,27 @@ int batch_device(const ccfj_batch_args& a, long long total, cudaStream_t s) {
     in[1] = InDesc{hb, a.nf, 1, nullptr};
   }
   BatchDev bd{};
-  const size_t esz = a.itype == 1 ? 8 : 4;
+  const float tau = a.tau > 0 ? a.tau : kDefaultTau32;
+  float* kb = nullptr;
+  if (a.itype == 1) {
+    kb = sc.get_n<float>(a.nf);
+    if (!kb) return CCFJ_ERR_ALLOC;
+    fj_kbounds_kernel<float><<<div_up(a.nf, 8), dim3(32, 8), 0, s>>>(a.f, a.c, a.nf, a.nc, tau, kb);
+    count_launch();
+    CCFJ_LAUNCH_CHECK("fj_kbounds_kernel");
+  }
+  const size_t esz = a.itype == 1 ? sizeof(StationCoef<float>) : 4;
   for (int j = 0; j < nin; ++j) {
     void* g = sc.get((size_t)total * a.nf * esz);
     if (!g) return CCFJ_ERR_ALLOC;
     batch_prep_u_kernel<<<dim3(div_up(total, 8), div_up(a.nf, 32)), dim3(32, 8), 0, s>>>(
-        in[j], a.offsets, a.nsets, total, a.nf, drs, wtr, a.itype, g);
+        in[j], a.offsets, a.nsets, total, a.nf, a.r, drs, wtr, geo, kb, a.itype, g);
     count_launch();
     CCFJ_LAUNCH_CHECK("batch_prep_u_kernel");
     bd.base.gb[j] = g;
   }
+  bd.base.kb = kb;
+  bd.base.geo = geo;
   bd.base.rs = a.r;
   bd.base.drs = drs;
   bd.base.f = a.f;
@@ -307,7 +322,7 @@ int batch_device(const ccfj_batch_args& a, long long total, cudaStream_t s) {
   bd.base.out = a.out;
   bd.base.nf = a.nf;
   bd.base.nc = a.nc;
-  bd.base.tau = a.tau > 0 ? a.tau : kDefaultTau32;
+  bd.base.tau = tau;
   bd.off = a.offsets;
   bd.order = order;
   bd.nsets = a.nsets;

@@ -66,14 +66,25 @@ template <>
 struct Cell<float> {
   float q_hi, q_lo;  // f / c as a double-float (cycles per unit distance)
   float k;           // 2 pi f / c
+  float k2;          // k^2
   float inv_k;
   float inv_k2;
+  // Set by prepare_folded() for the folded interval sum:
+  // s8 = 8 / k: x = k r >= 8 where r >= s8, and an interval of length D
+  // takes the closed form (k |D| >= tau) where |D| (8 / tau) >= s8.
+  float s8;
+  // The wavenumber exactly as init() rounds it (also used for the
+  // per-frequency bounds of the folded interval sum).
+  static __device__ __forceinline__ float wavenumber(float fl, float cl) {
+    return (float)(fjs::kTwoPi * ((double)fl / (double)cl));
+  }
   __device__ void init(float fl, float cl) {
     const double q = (double)fl / (double)cl;
     q_hi = (float)q;
     q_lo = (float)(q - (double)q_hi);
     const double kd = fjs::kTwoPi * q;
-    k = (float)kd;
+    k = wavenumber(fl, cl);
+    k2 = (float)(kd * kd);
     inv_k = (float)(1.0 / kd);
     inv_k2 = (float)(1.0 / (kd * kd));
   }
@@ -85,15 +96,52 @@ struct Cell<float> {
     const float p_lo = fmaf(q_lo, r, e);
     fjs::eval_station_f32<WJ, WY, WZ1>(x, p_hi, p_lo, need_b, J, Y);
   }
+  __device__ void prepare_folded() { s8 = (float)(8.0 / (fjs::kTwoPi * ((double)q_hi + (double)q_lo))); }
+  // gam = sqrt(2 / (pi k)): the Hankel amplitude is M = gam / sqrt(r).
+  __device__ __forceinline__ float gamma() const { return sqrtf((float)(2.0 / fjs::kPi) / k); }
+  // Station values for the folded interval sum: y0 = Z0 / M, y1 = Z1 / M
+  // with M = gam / sqrtr, and B itself. rinv = 1/r, sqrtr = sqrt(r) (both
+  // per station; sqrtr = 1 where r = 0). The range test uses s8, so x = k r
+  // is formed only below 8.
+  template <bool WJ, bool WY>
+  __device__ __forceinline__ void eval_scaled(float r, float rinv, float sqrtr, bool need_b,
+                                              ZB<float>& J, ZB<float>& Y) const {
+    if (r >= s8) {  // x >= 8
+      const float p_hi = q_hi * r;
+      const float e = fmaf(q_hi, r, -p_hi);
+      const float p_lo = fmaf(q_lo, r, e);
+      // M = sqrt(2 / (pi x)) = sqrt(s / (4 pi)), s = 8 / x
+      const float s = s8 * rinv;
+      const float m = need_b ? fjs::sqrt_fast(s * (float)(0.25 / fjs::kPi)) : 0.0f;
+      fjs::eval_large_scaled_f32<WJ, WY, true>(s, p_hi, p_lo, need_b, m, J, Y);
+    } else {
+      fjs::eval_small_f32<WJ, WY, true>(k * r, need_b, J, Y);
+      // 1 / M = sqrtr sqrt(pi k / 2) (sqrt(pi x / 2) for r > 0)
+      const float sc = sqrtr * fjs::sqrt_fast((float)(fjs::kPi / 2.0) * k);
+      if (WJ) {
+        J.z0 *= sc;
+        J.z1 *= sc;
+      }
+      if (WY) {
+        Y.z0 *= sc;
+        Y.z1 *= sc;
+      }
+    }
+  }
 };
 template <>
 struct Cell<double> {
-  double q, k, inv_k, inv_k2;
+  double q, k, k2, inv_k, inv_k2;
+  double s8;  // as Cell<float>
+  static __device__ __forceinline__ double wavenumber(float fl, float cl) {
+    return fjs::kTwoPi * ((double)fl / (double)cl);
+  }
   __device__ void init(float fl, float cl) {
     q = (double)fl / (double)cl;
-    k = fjs::kTwoPi * q;
+    k = wavenumber(fl, cl);
+    k2 = k * k;
     inv_k = 1.0 / k;
-    inv_k2 = 1.0 / (k * k);
+    inv_k2 = 1.0 / k2;
   }
   template <bool WJ, bool WY, bool WZ1>
   __device__ __forceinline__ void eval(double r, double x, bool need_b, ZB<double>& J,
@@ -101,18 +149,168 @@ struct Cell<double> {
     (void)need_b;
     fjs::eval_station_f64<WJ, WY, WZ1>(x, q * r, J, Y);
   }
+  __device__ void prepare_folded() { s8 = 8.0 / k; }
+  __device__ __forceinline__ double gamma() const { return sqrt(2.0 / (fjs::kPi * k)); }
+  // As Cell<float>::eval_scaled (values divided by M = gam / sqrtr).
+  template <bool WJ, bool WY>
+  __device__ __forceinline__ void eval_scaled(double r, double rinv, double sqrtr, bool need_b,
+                                              ZB<double>& J, ZB<double>& Y) const {
+    (void)rinv;
+    (void)need_b;
+    fjs::eval_station_f64<WJ, WY, true>(k * r, q * r, J, Y);
+    const double sc = sqrtr * sqrt(0.5 * fjs::kPi * k);
+    if (WJ) {
+      J.z0 *= sc;
+      J.z1 *= sc;
+    }
+    if (WY) {
+      Y.z0 *= sc;
+      Y.z1 *= sc;
+    }
+  }
 };
 
 struct FjDev {
   const float* rs;
   const float* drs;  // [nr + 1]: r_i - r_{i-1}, 0 at i = 0 and at i = nr
+  // [nr]: (r_i, r_{i+1} - r_i (0 for the last pair), 1/r_i, sqrt(r_i)), with
+  // 1/r = 0 and sqrt(r) = 1 where r = 0
+  const float4* geo;
+  // itype 1: StationCoef<T> [nr][nf] per input; itype 0: g * w [nr][nf]
   const void* gb[2];
+  const void* kb;    // itype 1: fold threshold per frequency (T), see fold_threshold
   const float* f;
   const float* c;
   float* out;
   int nr, nf, nc;
   float tau;
 };
+
+// ------------------------------------------------- folded interval sum
+// For an interval (A, B) of length D that takes the quintic Hermite rule,
+// the term g_A I0 + (b/k) I1 of the per-interval integral (see
+// fj_interval.cuh) is linear in the station values h, h', h'' with
+// coefficients k^n times quantities that do not depend on the velocity:
+//
+//   k (a1 h_A + b1 h_B) + k^2 (a2 h_A' + b2 h_B') + k^3 (a3 h_A'' + b3 h_B'')
+//   a1 = g_A D/2 + b D^2/10      b1 = g_A D/2 + 2 b D^2/5
+//   a2 = g_A D^2/10 + b D^3/60   b2 = -g_A D^2/10 - b D^3/12
+//   a3 = g_A D^3/120             b3 = (g_A D^3 + b D^4)/120
+//
+// Summed over the intervals, each station collects P_n = (a_n of the
+// interval to its right) + (b_n of the interval to its left), and with
+// x = k r, h = x Z0, h' = Z0 - x Z1, h'' = -Z1 - x Z0 the whole sum is
+//
+//   (1/k^2) sum = sum_s Z0(x_s) (A_s - k^2 C_s) - k Z1(x_s) B_s
+//   A = P1 r + P2,   B = P2 r + P3,   C = P3 r.
+//
+// A, B, C are formed once per (station, frequency) in FP64 (the
+// cancellation between neighbouring intervals happens there, exactly), so
+// the kernel's per-(station, velocity) work is the special functions plus
+// three FMAs. An interval is folded in when, at its frequency, it takes the
+// Hermite rule at the smallest k (under the Y-basis rule, the stricter one)
+// and k D stays below kFoldMax at the largest |k|; a folded interval that
+// takes the closed form for some velocity has its Hermite part subtracted
+// there again, and intervals not folded in are integrated explicitly.
+// kFoldMax bounds that subtraction: the Hermite terms grow like (k D)^4/120
+// relative to the interval's integral.
+constexpr float kFoldMax = 4.0f;
+
+// Per frequency: the interval length below which an interval is folded in,
+// min(tau / min k, kFoldMax / max |k|) over the velocities. Below tau / k
+// an interval takes the Hermite rule for wavenumber k.
+template <typename T>
+__device__ __forceinline__ T fold_threshold(T kmin, T kabs, T tau) {
+  return fmin(tau / kmin, T(kFoldMax) / kabs);
+}
+
+// Whether interval (rA, rA + D) is folded in at a frequency with fold
+// threshold thr: short enough, and not reaching closer to the origin than
+// its own length (where the Y basis needs the closed form). The
+// preparation and the kernels evaluate exactly this, so they agree.
+template <typename T>
+__device__ __forceinline__ bool folded_interval(T thr, T D, T rA) {
+  return fabs(D) < thr && !(D > rA);
+}
+
+// Per (station, frequency): the folded-sum coefficients divided by the
+// station's sqrt(r) (the r part of the Hankel amplitude; sqrt(r) := 1 where
+// r = 0), and the station's spectrum value g (from which an explicit
+// interval rebuilds its b).
+template <typename T>
+struct alignas(16) StationCoef {
+  T A, B, C, g;
+};
+static_assert(sizeof(StationCoef<float>) == 16, "one 16-byte load per station");
+
+__device__ __forceinline__ StationCoef<float> load_coef(const StationCoef<float>* p) {
+  const float4 v = __ldg(reinterpret_cast<const float4*>(p));
+  return {v.x, v.y, v.z, v.w};
+}
+__device__ __forceinline__ StationCoef<double> load_coef(const StationCoef<double>* p) {
+  const double2* q = reinterpret_cast<const double2*>(p);
+  const double2 v0 = __ldg(q), v1 = __ldg(q + 1);
+  return {v0.x, v0.y, v1.x, v1.y};
+}
+
+// b of the interval from g1 to g2: (g2 - g1) / max(D, 0.1) as
+// src/FJcpu.cpp:259-261, in the kernel's precision.
+template <typename T>
+__device__ __forceinline__ T interval_slope(T g1, T g2, float D) {
+  return (g2 - g1) / (T)fmaxf(D, 0.1f);
+}
+
+// Coefficients of station s with value g at r (sqrtr = geo.w), left
+// neighbour (gl, rl) at distance Dl (if has_l) and right neighbour gr at
+// distance Dr (if has_r); thr = the frequency's fold threshold.
+template <typename T>
+__device__ __forceinline__ StationCoef<T> station_coef(T g, T gl, T gr, bool has_l, bool has_r,
+                                                       float r, float rl, float Dl, float Dr,
+                                                       float sqrtr, T thr) {
+  double P1 = 0.0, P2 = 0.0, P3 = 0.0;
+  if (has_l && folded_interval<T>(thr, (T)Dl, (T)rl)) {  // s is B of (s-1, s)
+    const double ga = gl, b = interval_slope<T>(gl, g, Dl), D = Dl;
+    const double D2 = D * D, D3 = D2 * D;
+    P1 += 0.5 * ga * D + 0.4 * b * D2;
+    P2 -= 0.1 * ga * D2 + b * D3 / 12.0;
+    P3 += (ga * D3 + b * D3 * D) / 120.0;
+  }
+  if (has_r && folded_interval<T>(thr, (T)Dr, (T)r)) {  // s is A of (s, s+1)
+    const double ga = g, b = interval_slope<T>(g, gr, Dr), D = Dr;
+    const double D2 = D * D, D3 = D2 * D;
+    P1 += 0.5 * ga * D + 0.1 * b * D2;
+    P2 += 0.1 * ga * D2 + b * D3 / 60.0;
+    P3 += ga * D3 / 120.0;
+  }
+  const double rd = r, w = 1.0 / (double)sqrtr;
+  return {(T)((P1 * rd + P2) * w), (T)((P2 * rd + P3) * w), (T)(P3 * rd * w), g};
+}
+
+// Fold threshold per frequency (one warp per frequency).
+template <typename T>
+__global__ void fj_kbounds_kernel(const float* __restrict__ f, const float* __restrict__ c,
+                                  int nf, int nc, T tau, T* __restrict__ thr) {
+  const int fi = blockIdx.x * blockDim.y + threadIdx.y;
+  if (fi >= nf) return;
+  const float fl = f[fi];
+  T lo = T(INFINITY), hi = T(0);
+  for (int j = threadIdx.x; j < nc; j += 32) {
+    const T k = Cell<T>::wavenumber(fl, c[j]);
+    lo = fmin(lo, k);
+    hi = fmax(hi, fabs(k));
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  }
+  if (threadIdx.x == 0) thr[fi] = fold_threshold<T>(lo, hi, tau);
+}
+
+// Station geometry for the itype-1 kernels (see FjDev::geo).
+__device__ __forceinline__ float4 station_geometry(float r, float d_next) {
+  const bool pos = r > 0.0f;
+  return make_float4(r, d_next, pos ? 1.0f / r : 0.0f, pos ? sqrtf(r) : 1.0f);
+}
 
 // ------------------------------------------------------------ preparation
 // Gathers row perm[i] (or i) of one input, takes every u_cs-th element, and
@@ -148,6 +346,26 @@ __global__ void fj_prep_u_kernel(InDesc in, int nr, int nf, const float* __restr
   }
 }
 
+// itype 1: gathers rows perm[i-1], perm[i], perm[i+1] (or i-1, i, i+1) of
+// one input and writes station i's folded-sum coefficients.
+template <typename T>
+__global__ void fj_prep_coef_kernel(InDesc in, int nr, int nf, const float* __restrict__ rs,
+                                    const float* __restrict__ drs,
+                                    const float4* __restrict__ geo, const T* __restrict__ thr,
+                                    StationCoef<T>* __restrict__ dst) {
+  const int fi = blockIdx.y * blockDim.x + threadIdx.x;
+  const int i = blockIdx.x * blockDim.y + threadIdx.y;
+  if (fi >= nf || i >= nr) return;
+  const long long* perm = in.perm;
+  const long long col = (long long)fi * in.cs;
+  const bool hl = i > 0, hr = i + 1 < nr;
+  const T g = (T)in.p[(perm ? perm[i] : i) * in.ld + col];
+  const T gl = hl ? (T)in.p[(perm ? perm[i - 1] : i - 1) * in.ld + col] : T(0);
+  const T gr = hr ? (T)in.p[(perm ? perm[i + 1] : i + 1) * in.ld + col] : T(0);
+  dst[(long long)i * nf + fi] = station_coef<T>(g, gl, gr, hl, hr, rs[i], hl ? rs[i - 1] : 0.0f,
+                                                drs[i], drs[i + 1], geo[i].w, thr[fi]);
+}
+
 // ------------------------------------------------- station-amortised kernel
 // acc += g_{i-1} I0 + b_i I1 / k per input and basis (I1k = I1 / k); the
 // sum is formed with one FMA per term.
@@ -181,14 +399,15 @@ __device__ __forceinline__ void accumulate_station(T (&acc)[2], T g0, T g1, T zJ
   } else if (MODE == CCFJ_MODE_Y) {
     acc[0] = fjs::fmaT(g0, zY, acc[0]);
   } else {
+    using fjs::fmaT;
     if (MODE == CCFJ_MODE_J_MINUS_Y) {
-      acc[0] += g0 * zJ - g1 * zY;
+      acc[0] = fmaT(-g1, zY, fmaT(g0, zJ, acc[0]));
     } else if (MODE == CCFJ_MODE_ABS_J) {
-      acc[0] = fjs::fmaT(g0, zJ, acc[0]);
-      acc[1] = fjs::fmaT(g1, zJ, acc[1]);
-    } else {
-      acc[0] += g0 * zJ - g1 * zY;
-      acc[1] += g1 * zJ + g0 * zY;
+      acc[0] = fmaT(g0, zJ, acc[0]);
+      acc[1] = fmaT(g1, zJ, acc[1]);
+    } else {  // ABS_H: (J(u0) - Y(u1)) + i (J(u1) + Y(u0))
+      acc[0] = fmaT(-g1, zY, fmaT(g0, zJ, acc[0]));
+      acc[1] = fmaT(g0, zY, fmaT(g1, zJ, acc[1]));
     }
   }
 }
@@ -210,6 +429,76 @@ __device__ __forceinline__ bool closed_form(T dx, T x1, T tau) {
   return fabs(dx) >= tau || (IS_Y && dx > x1);
 }
 
+// I0, I1 of one interval between stations (xA, zA) and (xB, zB): the
+// closed form or the Hermite rule, minus the Hermite part already in the
+// folded sum when the interval was folded in.
+template <typename T>
+__device__ __forceinline__ void explicit_moments(T xA, const ZB<T>& zA, T xB, const ZB<T>& zB,
+                                                 T dx, bool closed, bool folded, T& I0, T& I1) {
+  const Station<T> sA = fjs::make_station(xA, zA);
+  const Station<T> sB = fjs::make_station(xB, zB);
+  fjs::interval_moments<T>(sA, sB, dx, closed, I0, I1);
+  if (closed && folded) {
+    T h0, h1;
+    fjs::interval_moments<T>(sA, sB, dx, false, h0, h1);
+    I0 -= h0;
+    I1 -= h1;
+  }
+}
+
+// Interval (A, B) of one cell for the bases that need explicit work
+// (exJ / exY; lcJ / lcY its closed-form flags), in the units of the folded
+// sums (output / gam). yA*, yB* are the stations' values from eval_scaled
+// (Z / M, and B), at rA, rB with sqrt(r) = sqA, sqB; gA*, gB* the stations'
+// spectrum values of inputs 0 and 1. Rarely taken: arguments and result by
+// value.
+template <typename T>
+struct Acc2 {
+  T v[2];
+};
+template <typename T>
+__device__ __forceinline__ ZB<T> unscale(const ZB<T>& y, T m) {
+  return ZB<T>{y.z0 * m, y.z1 * m, y.b};
+}
+template <int MODE, typename T>
+__device__ __forceinline__ Acc2<T> explicit_interval(const Cell<T>& cell, bool exJ, bool exY,
+                                                     bool lcJ, bool lcY, bool folded, T D, T rA,
+                                                     T sqA, T rB, T sqB, ZB<T> yAJ, ZB<T> yBJ,
+                                                     ZB<T> yAY, ZB<T> yBY, T gA0, T gB0, T gA1,
+                                                     T gB1) {
+  using T2 = typename Vec2<T>::type;
+  const T k = cell.k;
+  const T gam = cell.gamma();
+  const T mA = gam / sqA, mB = gam / sqB;
+  const T xA = k * rA, xB = k * rB, dx = k * D;
+  T2 g0, g1;
+  g0.x = gA0;
+  g0.y = interval_slope<T>(gA0, gB0, (float)D);
+  g1.x = gA1;
+  g1.y = ModeTraits<MODE>::NIN > 1 ? interval_slope<T>(gA1, gB1, (float)D) : T(0);
+  T I0J = 0, I1J = 0, I0Y = 0, I1Y = 0;
+  if (ModeTraits<MODE>::WJ && exJ)
+    explicit_moments<T>(xA, unscale(yAJ, mA), xB, unscale(yBJ, mB), dx, lcJ, folded, I0J, I1J);
+  if (ModeTraits<MODE>::WY && exY)
+    explicit_moments<T>(xA, unscale(yAY, mA), xB, unscale(yBY, mB), dx, lcY, folded, I0Y, I1Y);
+  const T inv_k = T(1) / k;
+  const T s0 = inv_k * inv_k / gam, s1 = s0 * inv_k;
+  T acc[2] = {T(0), T(0)};
+  accumulate_interval<MODE, T>(acc, g0, g1, I0J * s0, I1J * s1, I0Y * s0, I1Y * s1);
+  return Acc2<T>{{acc[0], acc[1]}};
+}
+
+// Minimum resident 256-thread CTAs per SM of the kernels built on
+// fj_cells. FP32: at most 64 registers, four CTAs (more warps to hide the
+// special functions' latency); the single-set and the batch kernels share
+// the bound, so they compile the cell loop alike and agree bit for bit.
+// FP64 cells hold twice the registers: a cap would only make them spill.
+#ifndef CCFJ_FJ_MIN_BLOCKS
+#define CCFJ_FJ_MIN_BLOCKS 4
+#endif
+template <typename T>
+constexpr int fj_min_blocks() { return sizeof(T) == 4 ? CCFJ_FJ_MIN_BLOCKS : 1; }
+
 // CPT cells (f, c), (f, c + 1), ... per thread share the per-station loads.
 // The transform of the CPT cells (fi, c0), (fi, c0 + 1), ... of one data
 // set; shared by the grid kernel below and the persistent batch kernel.
@@ -227,78 +516,97 @@ __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
   for (int j = 0; j < CPT; ++j) tot[j][0] = tot[j][1] = T(0);
   ZB<T> Jz{}, Yz{};
   if (ITYPE == 1) {
-    const T tau = (T)a.tau;
-    Station<T> sJp[CPT], sYp[CPT];
-    T xp[CPT];
-    T r_cur = (T)__ldg(a.rs);
-    T dr_next = (T)__ldg(a.drs + 1);  // drs has nr + 1 entries, the last 0
+    const T thr_fold = static_cast<const T*>(a.kb)[fi];
+    const StationCoef<T>* q0p = static_cast<const StationCoef<T>*>(a.gb[0]) + fi;
+    const StationCoef<T>* q1p = static_cast<const StationCoef<T>*>(a.gb[MT::NIN > 1 ? 1 : 0]) + fi;
+    const T d8 = T(8) / (T)a.tau;  // closed form where |D| d8 >= s8
+#pragma unroll
+    for (int j = 0; j < CPT; ++j) cell[j].prepare_folded();
+    // out = gam (sum_s y0 (A - k^2 C) - k sum_s y1 B) + the explicit intervals
+    T tot[CPT][2];
+    bool lnJ[CPT], lnY[CPT];   // closed form for interval (i, i+1), per basis
+    // The explicit path needs station i-1's values: single-basis modes carry
+    // them (3 registers per cell); two-basis modes, short of registers,
+    // evaluate station i-1 again when an explicit interval comes.
+    constexpr bool kCarry = !(WJ && WY);
+    ZB<T> zpJ[kCarry ? CPT : 1], zpY[kCarry ? CPT : 1];
 #pragma unroll
     for (int j = 0; j < CPT; ++j) {
-      xp[j] = cell[j].k * r_cur;
-      const bool nb = closed_form<T, WY>(cell[j].k * dr_next, xp[j], tau);  // Y rule: superset
-      cell[j].template eval<WJ, WY, true>(r_cur, xp[j], nb, Jz, Yz);
-      if (WJ) sJp[j] = fjs::make_station(xp[j], Jz);
-      if (WY) sYp[j] = fjs::make_station(xp[j], Yz);
+      tot[j][0] = tot[j][1] = T(0);
+      lnJ[j] = lnY[j] = false;
     }
-    // lnJ/lnY[j]: interval (i, i+1) of cell j takes the closed form in the
-    // J / Y basis (the Y rule also sends near-origin intervals there)
-    bool lnJ[CPT], lnY[CPT];
-#pragma unroll
-    for (int j = 0; j < CPT; ++j) {
-      lnJ[j] = closed_form<T, false>(cell[j].k * dr_next, xp[j], tau);
-      lnY[j] = closed_form<T, true>(cell[j].k * dr_next, xp[j], tau);
-    }
-    for (int i0 = 1; i0 < a.nr; i0 += kChunk) {
+    bool fold_next = true;  // "interval (-1, 0)" needs no explicit work
+    for (int i0 = 0; i0 < a.nr; i0 += kChunk) {
       const int i1 = min(a.nr, i0 + kChunk);
-      T acc[CPT][2];
+      T acc0[CPT][2], acc1[CPT][2];
 #pragma unroll
-      for (int j = 0; j < CPT; ++j) acc[j][0] = acc[j][1] = T(0);
+      for (int j = 0; j < CPT; ++j) acc0[j][0] = acc0[j][1] = acc1[j][0] = acc1[j][1] = T(0);
 #pragma unroll 2
       for (int i = i0; i < i1; ++i) {
-        const T r = (T)__ldg(a.rs + i);
-        const T dr = dr_next;
-        dr_next = (T)__ldg(a.drs + i + 1);
-        using T2 = typename Vec2<T>::type;
-        const long long gidx = (long long)i * a.nf + fi;
-        const T2 g0 = __ldg(static_cast<const T2*>(a.gb[0]) + gidx);
-        T2 g1;
-        if (MT::NIN > 1) g1 = __ldg(static_cast<const T2*>(a.gb[1]) + gidx);
+        const float4 gm = __ldg(a.geo + i);
+        const T r = gm.x, D_next = gm.y;  // D_next: interval (i, i+1)
+        const bool fold_cur = fold_next;
+        const bool near = D_next > r;     // interval (i, i+1) reaches near the origin
+        fold_next = folded_interval<T>(thr_fold, D_next, r);
+        const T dn8 = fabs(D_next) * d8;
+        const long long qi = (long long)i * a.nf;
+        const StationCoef<T> q0 = load_coef(q0p + qi);
+        StationCoef<T> q1{};
+        if (MT::NIN > 1) q1 = load_coef(q1p + qi);
 #pragma unroll
         for (int j = 0; j < CPT; ++j) {
-          const T x = cell[j].k * r;
-          const T dx = cell[j].k * dr;
           const bool lcJ = lnJ[j], lcY = lnY[j];
-          const T dxn = cell[j].k * dr_next;
-          if (WJ) lnJ[j] = closed_form<T, false>(dxn, x, tau);
-          if (WY) lnY[j] = closed_form<T, true>(dxn, x, tau);
+          const bool cl = dn8 >= cell[j].s8;
+          if (WJ) lnJ[j] = cl;
+          if (WY) lnY[j] = cl || near;  // Y0 is singular at 0
           // B is needed where an adjacent interval takes the closed form
           const bool nb = WY ? (lcY || lnY[j]) : (lcJ || lnJ[j]);
-          cell[j].template eval<WJ, WY, true>(r, x, nb, Jz, Yz);
-          T I0J = 0, I1J = 0, I0Y = 0, I1Y = 0;
-          if (WJ) {
-            const Station<T> sJ = fjs::make_station(x, Jz);
-            fjs::interval_moments<T>(sJp[j], sJ, dx, lcJ, I0J, I1J);
-            sJp[j] = sJ;
+          cell[j].template eval_scaled<WJ, WY>(r, (T)gm.z, (T)gm.w, nb, Jz, Yz);
+          const T u0 = fjs::fmaT(-cell[j].k2, q0.C, q0.A);
+          const T u1 = MT::NIN > 1 ? fjs::fmaT(-cell[j].k2, q1.C, q1.A) : T(0);
+          accumulate_station<MODE, T>(acc0[j], u0, u1, WJ ? Jz.z0 : T(0), WY ? Yz.z0 : T(0));
+          accumulate_station<MODE, T>(acc1[j], q0.B, q1.B, WJ ? Jz.z1 : T(0), WY ? Yz.z1 : T(0));
+          const bool exJ = WJ && (lcJ || !fold_cur), exY = WY && (lcY || !fold_cur);
+          if (exJ || exY) {
+            // interval (i-1, i) (never at i = 0)
+            const float4 gp = __ldg(a.geo + i - 1);
+            ZB<T> pJ{}, pY{};
+            if constexpr (kCarry) {
+              pJ = zpJ[j];
+              pY = zpY[j];
+            } else {
+              cell[j].template eval_scaled<WJ, WY>((T)gp.x, (T)gp.z, (T)gp.w, lcJ || lcY, pJ, pY);
+            }
+            const T gA0 = __ldg(&q0p[qi - a.nf].g);
+            const T gA1 = MT::NIN > 1 ? __ldg(&q1p[qi - a.nf].g) : T(0);
+            const Acc2<T> e = explicit_interval<MODE, T>(cell[j], exJ, exY, lcJ, lcY, fold_cur,
+                                                         (T)gp.y, (T)gp.x, (T)gp.w, r, (T)gm.w, pJ,
+                                                         Jz, pY, Yz, gA0, q0.g, gA1, q1.g);
+            acc0[j][0] += e.v[0];
+            acc0[j][1] += e.v[1];
           }
-          if (WY) {
-            const Station<T> sY = fjs::make_station(x, Yz);
-            fjs::interval_moments<T>(sYp[j], sY, dx, lcY, I0Y, I1Y);
-            sYp[j] = sY;
+          if constexpr (kCarry) {
+            if (WJ) zpJ[j] = Jz;
+            if (WY) zpY[j] = Yz;
           }
-          accumulate_interval<MODE, T>(acc[j], g0, g1, I0J, I1J * cell[j].inv_k, I0Y,
-                                       I1Y * cell[j].inv_k);
-          xp[j] = x;
         }
       }
 #pragma unroll
       for (int j = 0; j < CPT; ++j) {
-        tot[j][0] += acc[j][0];
-        tot[j][1] += acc[j][1];
+        tot[j][0] += fjs::fmaT(-cell[j].k, acc1[j][0], acc0[j][0]);
+        tot[j][1] += fjs::fmaT(-cell[j].k, acc1[j][1], acc0[j][1]);
       }
     }
 #pragma unroll
-    for (int j = 0; j < CPT; ++j)
-      if (c0 + j < a.nc) a.out[(long long)(c0 + j) * a.nf + fi] = finish<MODE, T>(tot[j], cell[j].inv_k2);
+    for (int j = 0; j < CPT; ++j) {
+      const T gam = cell[j].gamma();
+      T res[2];
+      res[0] = gam * tot[j][0];
+      res[1] = gam * tot[j][1];
+      // k = 0 (f = 0) divides by zero in the reference: NaN
+      const float v = cell[j].k == T(0) ? __int_as_float(0x7fffffff) : finish<MODE, T>(res, T(1));
+      if (c0 + j < a.nc) a.out[(long long)(c0 + j) * a.nf + fi] = v;
+    }
   } else {
     for (int i0 = 0; i0 < a.nr; i0 += kChunk) {
       const int i1 = min(a.nr, i0 + kChunk);

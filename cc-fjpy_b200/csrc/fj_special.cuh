@@ -76,6 +76,16 @@ FJ_HD float rsqrt_fast(float x) {
   return 1.0f / sqrtf(x);
 #endif
 }
+// sqrt by the SFU's approximation (one MUFU op, relative error ~1 ulp).
+FJ_HD float sqrt_fast(float x) {
+#ifdef __CUDA_ARCH__
+  float y;
+  asm("sqrt.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+#else
+  return sqrtf(x);
+#endif
+}
 FJ_HD float log_fast(float x) {
 #ifdef __CUDA_ARCH__
   return __logf(x);
@@ -149,51 +159,53 @@ FJ_HD void sincos_cycles_f32(float u, float& s, float& c) {
 }
 
 // ------------------------------------------ station evaluation, FP32
-// x: the argument (FP32, for the smooth parts and the range choice);
-// p_hi + p_lo: x / (2 pi) in cycles (double-float, for the phase).
-// WANT_J / WANT_Y select the basis, WANT_Z1 adds Z1 (the integral forms
-// need it, the trapezoid does not); B = int_0^x Z0 is computed only when
-// need_b (the closed form of a long interval next to this station needs it;
-// the Hermite rule of short intervals does not).
+// The x >= 8 range in Hankel form, returning the values divided by the
+// Hankel amplitude M = sqrt(2 / (pi x)): y0 = Z0 / M, y1 = Z1 / M, and B
+// itself (m = M is read only when need_b). s = 8 / x; p_hi + p_lo = x / (2 pi)
+// in cycles (double-float). Without the amplitude the four polynomials need
+// no scaling, and a caller that can fold M elsewhere (the folded interval
+// sum does) never forms it.
 template <bool WANT_J, bool WANT_Y, bool WANT_Z1>
-FJ_HD void eval_station_f32(float x, float p_hi, float p_lo, bool need_b, ZB<float>& J,
-                            ZB<float>& Y) {
-  if (x >= 8.0f) {
-    float sn, cs;
-    sincos_cycles_f32(chi_cycles_f32(p_hi, p_lo), sn, cs);
-    const float rs = rsqrt_fast(x);  // one MUFU op gives both 1/sqrt(x) and 1/x
-    const float s = 8.0f * (rs * rs);
-    const float z = s * s;
-    const float M = kSqrt2OverPiF * rs;
-    const float sM = s * M;
-    constexpr float cp0[] = FJC_F32_L_P0;
-    constexpr float cq0[] = FJC_F32_L_Q0;
-    const float P0 = horner(cp0, z) * M;
-    const float Q0 = horner(cq0, z) * sM;
-    float P1 = 0.f, Q1 = 0.f;
-    if (WANT_Z1) {
-      constexpr float cp1[] = FJC_F32_L_P1;
-      constexpr float cq1[] = FJC_F32_L_Q1;
-      P1 = horner(cp1, z) * M;
-      Q1 = horner(cq1, z) * sM;
-    }
-    if (WANT_J) {
-      J.z0 = fmaT(P0, cs, -Q0 * sn);
-      if (WANT_Z1) J.z1 = fmaT(P1, sn, Q1 * cs);
-    }
-    if (WANT_Y) {
-      Y.z0 = fmaT(P0, sn, Q0 * cs);
-      if (WANT_Z1) Y.z1 = fmaT(Q1, sn, -P1 * cs);
-    }
-    if (WANT_Z1 && need_b) {
-      constexpr float cr0[] = FJC_F32_L_RHO0;
-      constexpr float cr1[] = FJC_F32_L_RHO1;
-      const float rho0 = horner(cr0, z);
-      const float rho1 = horner(cr1, z) * s;
-      if (WANT_J) J.b = fmaT(J.z1, rho0, fmaT(-J.z0, rho1, 1.0f));
-      if (WANT_Y) Y.b = fmaT(Y.z1, rho0, -Y.z0 * rho1);
-    }
-  } else if (x >= 2.0f) {
+FJ_HD void eval_large_scaled_f32(float s, float p_hi, float p_lo, bool need_b, float m,
+                                 ZB<float>& J, ZB<float>& Y) {
+  float sn, cs;
+  sincos_cycles_f32(chi_cycles_f32(p_hi, p_lo), sn, cs);
+  const float z = s * s;
+  constexpr float cp0[] = FJC_F32_L_P0;
+  constexpr float cq0[] = FJC_F32_L_Q0;
+  const float P0 = horner(cp0, z);
+  const float Q0 = horner(cq0, z) * s;
+  float P1 = 0.f, Q1 = 0.f;
+  if (WANT_Z1) {
+    constexpr float cp1[] = FJC_F32_L_P1;
+    constexpr float cq1[] = FJC_F32_L_Q1;
+    P1 = horner(cp1, z);
+    Q1 = horner(cq1, z) * s;
+  }
+  if (WANT_J) {
+    J.z0 = fmaT(P0, cs, -Q0 * sn);
+    if (WANT_Z1) J.z1 = fmaT(P1, sn, Q1 * cs);
+  }
+  if (WANT_Y) {
+    Y.z0 = fmaT(P0, sn, Q0 * cs);
+    if (WANT_Z1) Y.z1 = fmaT(Q1, sn, -P1 * cs);
+  }
+  if (WANT_Z1 && need_b) {
+    constexpr float cr0[] = FJC_F32_L_RHO0;
+    constexpr float cr1[] = FJC_F32_L_RHO1;
+    const float rho0 = horner(cr0, z);
+    const float rho1 = horner(cr1, z) * s;
+    // B_J = 1 + J1 rho0 - J0 rho1, B_Y = Y1 rho0 - Y0 rho1 (Wronskian form)
+    if (WANT_J) J.b = fmaT(m, fmaT(J.z1, rho0, -J.z0 * rho1), 1.0f);
+    if (WANT_Y) Y.b = m * fmaT(Y.z1, rho0, -Y.z0 * rho1);
+  }
+}
+
+// The x < 8 ranges: polynomials in (x - xc) / 1.5 for 2 <= x < 8, and in
+// (x/2)^2 with the log term of Y for x < 2. Z0, Z1 and B themselves.
+template <bool WANT_J, bool WANT_Y, bool WANT_Z1>
+FJ_HD void eval_small_f32(float x, bool need_b, ZB<float>& J, ZB<float>& Y) {
+  if (x >= 2.0f) {
     const bool hi = x >= 5.0f;
     const float u = (x - (hi ? 6.5f : 3.5f)) * (1.0f / 1.5f);
     if (hi) {
@@ -280,6 +292,32 @@ FJ_HD void eval_station_f32(float x, float p_hi, float p_lo, bool need_b, ZB<flo
         }
       }
     }
+  }
+}
+
+// x: the argument (FP32, for the smooth parts and the range choice);
+// p_hi + p_lo: x / (2 pi) in cycles (double-float, for the phase).
+// WANT_J / WANT_Y select the basis, WANT_Z1 adds Z1 (the integral forms
+// need it, the trapezoid does not); B = int_0^x Z0 is computed only when
+// need_b (the closed form of a long interval next to this station needs it;
+// the Hermite rule of short intervals does not).
+template <bool WANT_J, bool WANT_Y, bool WANT_Z1>
+FJ_HD void eval_station_f32(float x, float p_hi, float p_lo, bool need_b, ZB<float>& J,
+                            ZB<float>& Y) {
+  if (x >= 8.0f) {
+    const float rs = rsqrt_fast(x);  // one MUFU op gives both 1/sqrt(x) and 1/x
+    const float M = kSqrt2OverPiF * rs;
+    eval_large_scaled_f32<WANT_J, WANT_Y, WANT_Z1>(8.0f * (rs * rs), p_hi, p_lo, need_b, M, J, Y);
+    if (WANT_J) {
+      J.z0 *= M;
+      if (WANT_Z1) J.z1 *= M;
+    }
+    if (WANT_Y) {
+      Y.z0 *= M;
+      if (WANT_Z1) Y.z1 *= M;
+    }
+  } else {
+    eval_small_f32<WANT_J, WANT_Y, WANT_Z1>(x, need_b, J, Y);
   }
 }
 

@@ -36,8 +36,9 @@ using fjs::Station;
 using fjs::ZB;
 
 // ------------------------------------------------------------ preparation
+// drs, wtr, and (if geo) the itype-1 station geometry.
 __global__ void fj_prep_geom_kernel(const float* __restrict__ rs, int nr, float* __restrict__ drs,
-                                    float* __restrict__ wtr) {
+                                    float* __restrict__ wtr, float4* __restrict__ geo) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i == nr) drs[nr] = 0.0f;  // padding read by the kernels' one-station lookahead
   if (i >= nr) return;
@@ -45,17 +46,15 @@ __global__ void fj_prep_geom_kernel(const float* __restrict__ rs, int nr, float*
   const float dl = i > 0 ? r - rs[i - 1] : 0.0f;
   const float dr = i + 1 < nr ? rs[i + 1] - r : 0.0f;
   drs[i] = dl;
+  if (geo) geo[i] = station_geometry(r, dr);
   // dr0 = fmaxf(r2 - r1, 0.1) per interval, as src/FJcpu.cpp:354
   const float w0 = i > 0 ? fmaxf(dl, 0.1f) : 0.0f;
   const float w1 = i + 1 < nr ? fmaxf(dr, 0.1f) : 0.0f;
   wtr[i] = (w0 + w1) * 0.5f * r;
 }
 
-#ifndef CCFJ_FJ_MIN_BLOCKS
-#define CCFJ_FJ_MIN_BLOCKS 1
-#endif
 template <int MODE, int ITYPE, typename T, int CPT>
-__global__ void __launch_bounds__(256, CCFJ_FJ_MIN_BLOCKS) fj_amortized_kernel(FjDev a) {
+__global__ void __launch_bounds__(256, fj_min_blocks<T>()) fj_amortized_kernel(FjDev a) {
   fj_cells<MODE, ITYPE, T, CPT>(a, blockIdx.x * blockDim.x + threadIdx.x,
                                 (blockIdx.y * blockDim.y + threadIdx.y) * CPT);
 }
@@ -128,7 +127,7 @@ __global__ void __launch_bounds__(256) fj_plain64_kernel(FjDev a, const float* g
 }
 
 void fj_prep_geom_kernel_shared(const float* rs, int nr, float* drs, float* wtr, cudaStream_t s) {
-  fj_prep_geom_kernel<<<div_up(nr + 1, 256), 256, 0, s>>>(rs, nr, drs, wtr);
+  fj_prep_geom_kernel<<<div_up(nr + 1, 256), 256, 0, s>>>(rs, nr, drs, wtr, nullptr);
 }
 
 // Gathered plain copy of one input, [nr][nf] float (for the comparator).
@@ -247,13 +246,8 @@ long long tune_key(const ccfj_fj_args& a) {
 // two-input Bessel form and the trapezoid, one for the two-basis forms
 // (their register use leaves too few warps resident with more).
 int default_cpt_for(int mode, int itype) {
-  if (itype == 0) return 4;
-  switch (mode) {
-    case CCFJ_MODE_J:
-    case CCFJ_MODE_Y: return 2;
-    case CCFJ_MODE_ABS_J: return 4;
-    default: return 1;
-  }
+  (void)mode;  // under the 64-register cap 2 velocities win (or tie) in every mode
+  return itype == 0 ? 4 : 2;
 }
 
 int tuned_cpt(const ccfj_fj_args& a) {
@@ -267,20 +261,83 @@ void record_tuned_cpt(const ccfj_fj_args& a, int cpt) {
   g_tune[tune_key(a)] = cpt;
 }
 
+// Bytes of the itype-1 per-station geometry and per-frequency fold
+// thresholds, and of one input's interval data.
+size_t geometry_bytes(const ccfj_fj_args& a) {
+  return a.itype == 1 ? sizeof(float4) * (size_t)a.nr : 0;
+}
+size_t kbounds_bytes(const ccfj_fj_args& a) {
+  return a.itype == 1 ? (a.precision == CCFJ_PREC_FP32 ? 4 : 8) * (size_t)a.nf : 0;
+}
+size_t interval_data_bytes(const ccfj_fj_args& a) {
+  const size_t t = a.precision == CCFJ_PREC_FP32 ? 4 : 8;
+  return (size_t)a.nr * a.nf * (a.itype == 1 ? 4 * t : t);
+}
+
+// Fills d.kb (itype 1) and d.gb[0..nin) from the inputs: the per-frequency
+// fold thresholds and the station coefficients of the folded interval sum
+// (itype 1), or g * w (itype 0). kb and gbuf[] are device buffers of the
+// sizes above; d.rs, d.drs, d.geo (itype 1), d.nr, d.nf, d.tau must be set.
+int prep_interval_data(const ccfj_fj_args& a, FjDev& d, const InDesc* in, int nin, void* kb,
+                       void* const* gbuf, const float* wtr, cudaStream_t s) {
+  const bool fp32 = a.precision == CCFJ_PREC_FP32;
+  if (a.itype == 1) {
+    const dim3 kbb(32, 8);
+    if (fp32)
+      fj_kbounds_kernel<float><<<div_up(a.nf, 8), kbb, 0, s>>>(a.f, a.c, a.nf, a.nc, d.tau,
+                                                               static_cast<float*>(kb));
+    else
+      fj_kbounds_kernel<double><<<div_up(a.nf, 8), kbb, 0, s>>>(a.f, a.c, a.nf, a.nc,
+                                                                (double)d.tau,
+                                                                static_cast<double*>(kb));
+    count_launch();
+    CCFJ_LAUNCH_CHECK("fj_kbounds_kernel");
+    d.kb = kb;
+  }
+  const dim3 pb(32, 8), pg(div_up(a.nr, 8), div_up(a.nf, 32));
+  for (int j = 0; j < nin; ++j) {
+    void* g = gbuf[j];
+    if (a.itype == 1) {
+      if (fp32)
+        fj_prep_coef_kernel<float><<<pg, pb, 0, s>>>(in[j], a.nr, a.nf, d.rs, d.drs, d.geo,
+                                                     static_cast<const float*>(kb),
+                                                     static_cast<StationCoef<float>*>(g));
+      else
+        fj_prep_coef_kernel<double><<<pg, pb, 0, s>>>(in[j], a.nr, a.nf, d.rs, d.drs, d.geo,
+                                                      static_cast<const double*>(kb),
+                                                      static_cast<StationCoef<double>*>(g));
+      count_launch();
+      CCFJ_LAUNCH_CHECK("fj_prep_coef_kernel");
+    } else {
+      if (fp32)
+        fj_prep_u_kernel<float><<<pg, pb, 0, s>>>(in[j], a.nr, a.nf, d.drs, wtr, 0, g);
+      else
+        fj_prep_u_kernel<double><<<pg, pb, 0, s>>>(in[j], a.nr, a.nf, d.drs, wtr, 0, g);
+      count_launch();
+      CCFJ_LAUNCH_CHECK("fj_prep_u_kernel");
+    }
+    d.gb[j] = g;
+  }
+  return CCFJ_OK;
+}
+
 // Device-resident transform: every pointer in `a` is a device pointer.
 int fj_device(const ccfj_fj_args& a, cudaStream_t s) {
   const int nin = nin_of(a.mode);
   Scratch sc(s);
   float* drs = sc.get_n<float>(a.nr + 1);
   float* wtr = sc.get_n<float>(a.nr);
-  if (!drs || !wtr) return CCFJ_ERR_ALLOC;
-  fj_prep_geom_kernel<<<div_up(a.nr + 1, 256), 256, 0, s>>>(a.r, a.nr, drs, wtr);
+  const bool folded = a.itype == 1 && a.precision != CCFJ_PREC_FP64_PLAIN;
+  float4* geo = folded ? sc.get_n<float4>(a.nr) : nullptr;
+  if (!drs || !wtr || (folded && !geo)) return CCFJ_ERR_ALLOC;
+  fj_prep_geom_kernel<<<div_up(a.nr + 1, 256), 256, 0, s>>>(a.r, a.nr, drs, wtr, geo);
   count_launch();
   CCFJ_LAUNCH_CHECK("fj_prep_geom_kernel");
 
   FjDev d{};
   d.rs = a.r;
   d.drs = drs;
+  d.geo = geo;
   d.f = a.f;
   d.c = a.c;
   d.out = a.out;
@@ -303,27 +360,29 @@ int fj_device(const ccfj_fj_args& a, cudaStream_t s) {
   }
 
   const float* plain[2] = {nullptr, nullptr};
-  const dim3 pb(32, 8), pg(div_up(a.nr, 8), div_up(a.nf, 32));
-  for (int j = 0; j < nin; ++j) {
-    if (a.precision == CCFJ_PREC_FP64_PLAIN) {
+  if (a.precision == CCFJ_PREC_FP64_PLAIN) {
+    const dim3 pb(32, 8), pg(div_up(a.nr, 8), div_up(a.nf, 32));
+    for (int j = 0; j < nin; ++j) {
       float* g = sc.get_n<float>((size_t)a.nr * a.nf);
       if (!g) return CCFJ_ERR_ALLOC;
       fj_gather_kernel<<<pg, pb, 0, s>>>(in[j], a.nr, a.nf, g);
       count_launch();
       CCFJ_LAUNCH_CHECK("fj_gather_kernel");
       plain[j] = g;
-      continue;
     }
-    const size_t esz = (a.precision == CCFJ_PREC_FP32 ? 4 : 8) * (a.itype == 1 ? 2 : 1);
-    void* g = sc.get((size_t)a.nr * a.nf * esz);
-    if (!g) return CCFJ_ERR_ALLOC;
-    if (a.precision == CCFJ_PREC_FP32)
-      fj_prep_u_kernel<float><<<pg, pb, 0, s>>>(in[j], a.nr, a.nf, drs, wtr, a.itype, g);
-    else
-      fj_prep_u_kernel<double><<<pg, pb, 0, s>>>(in[j], a.nr, a.nf, drs, wtr, a.itype, g);
-    count_launch();
-    CCFJ_LAUNCH_CHECK("fj_prep_u_kernel");
-    d.gb[j] = g;
+  } else {
+    void* kb = nullptr;
+    if (a.itype == 1) {
+      kb = sc.get(kbounds_bytes(a));
+      if (!kb) return CCFJ_ERR_ALLOC;
+    }
+    void* gbuf[2] = {nullptr, nullptr};
+    for (int j = 0; j < nin; ++j) {
+      gbuf[j] = sc.get(interval_data_bytes(a));
+      if (!gbuf[j]) return CCFJ_ERR_ALLOC;
+    }
+    const int st = prep_interval_data(a, d, in, nin, kb, gbuf, wtr, s);
+    if (st != CCFJ_OK) return st;
   }
 
   const int cpt = g_force_cpt > 0 ? g_force_cpt : tuned_cpt(a);
@@ -682,15 +741,18 @@ static int fj_noalloc(const ccfj_fj_args& a, cudaStream_t s) {
                      "spectrum as u[1]");
   const int nin = nin_of(a.mode);
   const size_t geom = round256(sizeof(float) * ((size_t)a.nr + 1));
-  const size_t per_input = round256((size_t)a.nr * a.nf * (a.itype == 1 ? 8 : 4));
-  const size_t need = 2 * geom + nin * per_input;
+  const size_t gbytes = round256(geometry_bytes(a));
+  const size_t kbytes = round256(kbounds_bytes(a));
+  const size_t per_input = round256(interval_data_bytes(a));
+  const size_t fixed = 2 * geom + gbytes + kbytes;
+  const size_t need = fixed + nin * per_input;
   if (need > kNoAllocScratchBytes)
     return set_error(CCFJ_ERR_INVALID,
                      "ccfj_fj_noalloc_v1: nr=%d nf=%d (%d input%s, itype %d) needs %zu bytes of "
                      "scratch; the fixed scratch holds %zu bytes (nr*nf up to about %zu for one "
                      "itype-1 input)",
                      a.nr, a.nf, nin, nin > 1 ? "s" : "", a.itype, need, kNoAllocScratchBytes,
-                     (kNoAllocScratchBytes - 2 * geom) / 8);
+                     (kNoAllocScratchBytes - fixed) / 16);
   void* base = nullptr;
   int st = noalloc_scratch_address(&base);
   if (st != CCFJ_OK) return st;
@@ -699,13 +761,15 @@ static int fj_noalloc(const ccfj_fj_args& a, cudaStream_t s) {
   // kernels of this call, so nothing needs clearing between calls.
   float* drs = reinterpret_cast<float*>(p);
   float* wtr = reinterpret_cast<float*>(p + geom);
-  fj_prep_geom_kernel<<<div_up(a.nr + 1, 256), 256, 0, s>>>(a.r, a.nr, drs, wtr);
+  float4* geo = a.itype == 1 ? reinterpret_cast<float4*>(p + 2 * geom) : nullptr;
+  fj_prep_geom_kernel<<<div_up(a.nr + 1, 256), 256, 0, s>>>(a.r, a.nr, drs, wtr, geo);
   count_launch();
   CCFJ_LAUNCH_CHECK("fj_prep_geom_kernel");
 
   FjDev d{};
   d.rs = a.r;
   d.drs = drs;
+  d.geo = geo;
   d.f = a.f;
   d.c = a.c;
   d.out = a.out;
@@ -713,16 +777,16 @@ static int fj_noalloc(const ccfj_fj_args& a, cudaStream_t s) {
   d.nf = a.nf;
   d.nc = a.nc;
   d.tau = a.tau > 0 ? a.tau : kDefaultTau32;
-  const dim3 pb(32, 8), pg(div_up(a.nr, 8), div_up(a.nf, 32));
+  InDesc in[2];
+  void* gbuf[2] = {nullptr, nullptr};
   for (int j = 0; j < nin; ++j) {
-    void* g = p + 2 * geom + j * per_input;
-    const InDesc in{a.u[j] + (long long)a.col_begin * a.fstride * a.u_es, a.u_ld,
-                    (long long)a.u_es * a.fstride, a.perm};
-    fj_prep_u_kernel<float><<<pg, pb, 0, s>>>(in, a.nr, a.nf, drs, wtr, a.itype, g);
-    count_launch();
-    CCFJ_LAUNCH_CHECK("fj_prep_u_kernel");
-    d.gb[j] = g;
+    in[j] = InDesc{a.u[j] + (long long)a.col_begin * a.fstride * a.u_es, a.u_ld,
+                   (long long)a.u_es * a.fstride, a.perm};
+    gbuf[j] = p + fixed + j * per_input;
   }
+  st = prep_interval_data(a, d, in, nin, a.itype == 1 ? p + 2 * geom + gbytes : nullptr, gbuf,
+                          wtr, s);
+  if (st != CCFJ_OK) return st;
   const int cpt = g_force_cpt > 0 ? g_force_cpt : tuned_cpt(a);
   switch (a.mode) {
     case CCFJ_MODE_J:

@@ -1,5 +1,11 @@
 """The ragged batch (many subarrays, one persistent launch) equals fj_noise
-called once per subarray, and matches the FP64 oracle."""
+called once per subarray, and matches the FP64 oracle.
+
+The batch and the single-set kernels run the same cell loop but are
+separate kernels, and the code generator may fuse a multiply and an add
+into one FMA in one of them and not in the other; so they agree to FP32
+rounding (SAME_TOL on the normalised spectra, with identical NaN
+positions), not bit for bit."""
 import ctypes
 import warnings
 
@@ -11,6 +17,7 @@ import fj_oracle as O
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-4
+SAME_TOL = 2e-6
 
 
 def _sets(seed, nsets, lo, hi, f):
@@ -36,7 +43,8 @@ def test_batch_equals_per_set_calls(itype, func):
         outs = ccfj.fj_noise_batch(ufs, rs, c, f, itype=itype, func=func)
         for uf, r, y in zip(ufs, rs, outs):
             single = ccfj.fj_noise(uf, r, c, f, itype=itype, func=func)
-            assert np.array_equal(y, single, equal_nan=True)
+            assert np.array_equal(np.isnan(y), np.isnan(single))
+            assert np.nanmax(np.abs(y.astype(np.float64) - single)) <= SAME_TOL
             y64 = O.fj_noise(uf, r, c, f, itype=itype, func=func)
             assert O.rel_error(y, y64) <= TOL
 
