@@ -19,6 +19,12 @@ using fjs::ZB;
 constexpr float kDefaultTau32 = 0.6f;
 constexpr float kDefaultTau64 = 0.05f;
 constexpr int kChunk = 64;           // stations per partial sum
+// Unroll factor of the itype-1 station loop.
+#ifndef CCFJ_STATION_UNROLL
+#define CCFJ_STATION_UNROLL 1
+#endif
+#define CCFJ_PRAGMA_(x) _Pragma(#x)
+#define CCFJ_PRAGMA(x) CCFJ_PRAGMA_(x)
 
 template <int MODE>
 struct ModeTraits;
@@ -100,23 +106,20 @@ struct Cell<float> {
   // gam = sqrt(2 / (pi k)): the Hankel amplitude is M = gam / sqrt(r).
   __device__ __forceinline__ float gamma() const { return sqrtf((float)(2.0 / fjs::kPi) / k); }
   // Station values for the folded interval sum: y0 = Z0 / M, y1 = Z1 / M
-  // with M = gam / sqrtr, and B itself. rinv = 1/r, sqrtr = sqrt(r) (both
-  // per station; sqrtr = 1 where r = 0). The range test uses s8, so x = k r
-  // is formed only below 8.
-  template <bool WJ, bool WY>
-  __device__ __forceinline__ void eval_scaled(float r, float rinv, float sqrtr, bool need_b,
-                                              ZB<float>& J, ZB<float>& Y) const {
-    if (r >= s8) {  // x >= 8
+  // with M = gam / sqrtr (rinv = 1/r and sqrtr = sqrt(r) per station;
+  // sqrtr = 1 where r = 0). The range test uses s8, so x = k r is formed
+  // only below 8; LARGE asserts x >= 8 and drops the test. B is not formed.
+  template <bool WJ, bool WY, bool LARGE>
+  __device__ __forceinline__ void eval_y(float r, float rinv, float sqrtr, ZB<float>& J,
+                                         ZB<float>& Y) const {
+    if (LARGE || r >= s8) {  // x >= 8
       const float p_hi = q_hi * r;
       const float e = fmaf(q_hi, r, -p_hi);
       const float p_lo = fmaf(q_lo, r, e);
-      // M = sqrt(2 / (pi x)) = sqrt(s / (4 pi)), s = 8 / x
-      const float s = s8 * rinv;
-      const float m = need_b ? fjs::sqrt_fast(s * (float)(0.25 / fjs::kPi)) : 0.0f;
-      fjs::eval_large_scaled_f32<WJ, WY, true>(s, p_hi, p_lo, need_b, m, J, Y);
+      fjs::eval_large_scaled_f32<WJ, WY, true>(s8 * rinv, p_hi, p_lo, false, 0.0f, J, Y);
     } else {
-      fjs::eval_small_f32<WJ, WY, true>(k * r, need_b, J, Y);
-      // 1 / M = sqrtr sqrt(pi k / 2) (sqrt(pi x / 2) for r > 0)
+      fjs::eval_small_f32<WJ, WY, true>(k * r, false, J, Y);
+      // 1 / M = sqrtr sqrt(pi k / 2) (= sqrt(pi x / 2) for r > 0)
       const float sc = sqrtr * fjs::sqrt_fast((float)(fjs::kPi / 2.0) * k);
       if (WJ) {
         J.z0 *= sc;
@@ -126,6 +129,29 @@ struct Cell<float> {
         Y.z0 *= sc;
         Y.z1 *= sc;
       }
+    }
+  }
+  // B = int_0^x Z0 at a station whose eval_y values are in J / Y (only the
+  // closed form of an interval needs it).
+  template <bool WJ, bool WY>
+  __device__ __forceinline__ void fill_b(float r, float rinv, ZB<float>& J, ZB<float>& Y) const {
+    if (r >= s8) {
+      // B_J = 1 + M (y1 rho0 - y0 rho1), B_Y = M (y1 rho0 - y0 rho1) with
+      // M = sqrt(s / (4 pi)), s = 8 / x
+      const float s = s8 * rinv;
+      const float z = s * s;
+      constexpr float cr0[] = FJC_F32_L_RHO0;
+      constexpr float cr1[] = FJC_F32_L_RHO1;
+      const float rho0 = fjs::horner(cr0, z);
+      const float rho1 = fjs::horner(cr1, z) * s;
+      const float m = fjs::sqrt_fast(s * (float)(0.25 / fjs::kPi));
+      if (WJ) J.b = fmaf(m, fmaf(J.z1, rho0, -J.z0 * rho1), 1.0f);
+      if (WY) Y.b = m * fmaf(Y.z1, rho0, -Y.z0 * rho1);
+    } else {
+      ZB<float> tJ{}, tY{};
+      fjs::eval_small_f32<WJ, WY, true>(k * r, true, tJ, tY);
+      J.b = tJ.b;
+      Y.b = tY.b;
     }
   }
 };
@@ -151,13 +177,12 @@ struct Cell<double> {
   }
   __device__ void prepare_folded() { s8 = 8.0 / k; }
   __device__ __forceinline__ double gamma() const { return sqrt(2.0 / (fjs::kPi * k)); }
-  // As Cell<float>::eval_scaled (values divided by M = gam / sqrtr).
-  template <bool WJ, bool WY>
-  __device__ __forceinline__ void eval_scaled(double r, double rinv, double sqrtr, bool need_b,
-                                              ZB<double>& J, ZB<double>& Y) const {
+  // As Cell<float>::eval_y / fill_b (values divided by M = gam / sqrtr).
+  template <bool WJ, bool WY, bool LARGE>
+  __device__ __forceinline__ void eval_y(double r, double rinv, double sqrtr, ZB<double>& J,
+                                         ZB<double>& Y) const {
     (void)rinv;
-    (void)need_b;
-    fjs::eval_station_f64<WJ, WY, true>(k * r, q * r, J, Y);
+    fjs::eval_station_f64<WJ, WY, false>(k * r, q * r, J, Y);
     const double sc = sqrtr * sqrt(0.5 * fjs::kPi * k);
     if (WJ) {
       J.z0 *= sc;
@@ -167,6 +192,15 @@ struct Cell<double> {
       Y.z0 *= sc;
       Y.z1 *= sc;
     }
+  }
+  template <bool WJ, bool WY>
+  __device__ __forceinline__ void fill_b(double r, double rinv, ZB<double>& J,
+                                         ZB<double>& Y) const {
+    (void)rinv;
+    ZB<double> tJ{}, tY{};
+    fjs::eval_station_f64<WJ, WY, true>(k * r, q * r, tJ, tY);
+    J.b = tJ.b;
+    Y.b = tY.b;
   }
 };
 
@@ -499,6 +533,11 @@ __device__ __forceinline__ Acc2<T> explicit_interval(const Cell<T>& cell, bool e
 template <typename T>
 constexpr int fj_min_blocks() { return sizeof(T) == 4 ? CCFJ_FJ_MIN_BLOCKS : 1; }
 
+template <bool B>
+struct BoolTag {
+  static constexpr bool value = B;
+};
+
 // CPT cells (f, c), (f, c + 1), ... per thread share the per-station loads.
 // The transform of the CPT cells (fi, c0), (fi, c0 + 1), ... of one data
 // set; shared by the grid kernel below and the persistent batch kernel.
@@ -506,7 +545,12 @@ template <int MODE, int ITYPE, typename T, int CPT>
 __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
   using MT = ModeTraits<MODE>;
   constexpr bool WJ = MT::WJ, WY = MT::WY;
-  if (fi >= a.nf || c0 >= a.nc) return;
+  // c0 is uniform across a warp (its lanes are 32 frequencies); lanes past
+  // the last frequency compute the last one and store nothing, so that all
+  // 32 lanes stay active for the warp-wide steps below
+  if (c0 >= a.nc) return;
+  const bool f_valid = fi < a.nf;
+  fi = f_valid ? fi : a.nf - 1;
   Cell<T> cell[CPT];
   const float fl = a.f[fi];
 #pragma unroll
@@ -519,77 +563,93 @@ __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
     const T thr_fold = static_cast<const T*>(a.kb)[fi];
     const StationCoef<T>* q0p = static_cast<const StationCoef<T>*>(a.gb[0]) + fi;
     const StationCoef<T>* q1p = static_cast<const StationCoef<T>*>(a.gb[MT::NIN > 1 ? 1 : 0]) + fi;
-    const T d8 = T(8) / (T)a.tau;  // closed form where |D| d8 >= s8
+    const T d8 = T(8) / (T)a.tau;  // closed form where |D| d8 >= s8 (k |D| >= tau)
+    T s8w = T(0);                  // largest s8 = 8 / k of the warp
 #pragma unroll
-    for (int j = 0; j < CPT; ++j) cell[j].prepare_folded();
-    // out = gam (sum_s y0 (A - k^2 C) - k sum_s y1 B) + the explicit intervals
-    T tot[CPT][2];
-    bool lnJ[CPT], lnY[CPT];   // closed form for interval (i, i+1), per basis
+    for (int j = 0; j < CPT; ++j) {
+      cell[j].prepare_folded();
+      s8w = fmax(s8w, cell[j].s8);
+    }
+    for (int o = 16; o > 0; o >>= 1) s8w = fmax(s8w, __shfl_xor_sync(0xffffffffu, s8w, o));
     // The explicit path needs station i-1's values: single-basis modes carry
-    // them (3 registers per cell); two-basis modes, short of registers,
+    // them (2 registers per cell); two-basis modes, short of registers,
     // evaluate station i-1 again when an explicit interval comes.
     constexpr bool kCarry = !(WJ && WY);
     ZB<T> zpJ[kCarry ? CPT : 1], zpY[kCarry ? CPT : 1];
+    // State of interval (i-1, i): length D, folded in, reaches near the
+    // origin. Station 0 has no such interval.
+    T D = T(0);
+    bool fold_cur = true, near_cur = false;
+    T acc0[CPT][2], acc1[CPT][2];
+    // One station: out += gam (y0 (A - k^2 C) - k y1 B), plus the explicit
+    // interval (i-1, i) where it is not (only) in the folded sum.
+    auto station = [&](auto large_tag, int i) {
+      constexpr bool LARGE = decltype(large_tag)::value;
+      const float4 gm = __ldg(a.geo + i);
+      const T r = gm.x, D_next = gm.y;
+      const long long qi = (long long)i * a.nf;
+      const StationCoef<T> q0 = load_coef(q0p + qi);
+      StationCoef<T> q1{};
+      if (MT::NIN > 1) q1 = load_coef(q1p + qi);
+      const T dl8 = fabs(D) * d8;
 #pragma unroll
-    for (int j = 0; j < CPT; ++j) {
-      tot[j][0] = tot[j][1] = T(0);
-      lnJ[j] = lnY[j] = false;
-    }
-    bool fold_next = true;  // "interval (-1, 0)" needs no explicit work
+      for (int j = 0; j < CPT; ++j) {
+        ZB<T> Jz{}, Yz{};
+        cell[j].template eval_y<WJ, WY, LARGE>(r, (T)gm.z, (T)gm.w, Jz, Yz);
+        const T u0 = fjs::fmaT(-cell[j].k2, q0.C, q0.A);
+        const T u1 = MT::NIN > 1 ? fjs::fmaT(-cell[j].k2, q1.C, q1.A) : T(0);
+        accumulate_station<MODE, T>(acc0[j], u0, u1, WJ ? Jz.z0 : T(0), WY ? Yz.z0 : T(0));
+        accumulate_station<MODE, T>(acc1[j], q0.B, q1.B, WJ ? Jz.z1 : T(0), WY ? Yz.z1 : T(0));
+        const bool clJ = dl8 >= cell[j].s8;
+        const bool clY = clJ || near_cur;  // Y0 is singular at 0
+        const bool exJ = WJ && (clJ || !fold_cur), exY = WY && (clY || !fold_cur);
+        if (i > 0 && (exJ || exY)) {
+          const float4 gp = __ldg(a.geo + i - 1);
+          ZB<T> pJ{}, pY{};
+          if constexpr (kCarry) {
+            pJ = zpJ[j];
+            pY = zpY[j];
+          } else {
+            cell[j].template eval_y<WJ, WY, false>((T)gp.x, (T)gp.z, (T)gp.w, pJ, pY);
+          }
+          // B at both ends where the interval takes the closed form
+          if ((WJ && exJ && clJ) || (WY && exY && clY)) {
+            cell[j].template fill_b<WJ, WY>((T)gp.x, (T)gp.z, pJ, pY);
+            cell[j].template fill_b<WJ, WY>(r, (T)gm.z, Jz, Yz);
+          }
+          const T gA0 = __ldg(&q0p[qi - a.nf].g);
+          const T gA1 = MT::NIN > 1 ? __ldg(&q1p[qi - a.nf].g) : T(0);
+          const Acc2<T> e = explicit_interval<MODE, T>(cell[j], exJ, exY, clJ, clY, fold_cur, D,
+                                                       (T)gp.x, (T)gp.w, r, (T)gm.w, pJ, Jz, pY,
+                                                       Yz, gA0, q0.g, gA1, q1.g);
+          acc0[j][0] += e.v[0];
+          acc0[j][1] += e.v[1];
+        }
+        if constexpr (kCarry) {
+          if (WJ) zpJ[j] = Jz;
+          if (WY) zpY[j] = Yz;
+        }
+      }
+      fold_cur = folded_interval<T>(thr_fold, D_next, r);
+      near_cur = D_next > r;
+      D = D_next;
+    };
+    const int lane = threadIdx.x & 31;
     for (int i0 = 0; i0 < a.nr; i0 += kChunk) {
       const int i1 = min(a.nr, i0 + kChunk);
-      T acc0[CPT][2], acc1[CPT][2];
 #pragma unroll
       for (int j = 0; j < CPT; ++j) acc0[j][0] = acc0[j][1] = acc1[j][0] = acc1[j][1] = T(0);
-#pragma unroll 2
-      for (int i = i0; i < i1; ++i) {
-        const float4 gm = __ldg(a.geo + i);
-        const T r = gm.x, D_next = gm.y;  // D_next: interval (i, i+1)
-        const bool fold_cur = fold_next;
-        const bool near = D_next > r;     // interval (i, i+1) reaches near the origin
-        fold_next = folded_interval<T>(thr_fold, D_next, r);
-        const T dn8 = fabs(D_next) * d8;
-        const long long qi = (long long)i * a.nf;
-        const StationCoef<T> q0 = load_coef(q0p + qi);
-        StationCoef<T> q1{};
-        if (MT::NIN > 1) q1 = load_coef(q1p + qi);
-#pragma unroll
-        for (int j = 0; j < CPT; ++j) {
-          const bool lcJ = lnJ[j], lcY = lnY[j];
-          const bool cl = dn8 >= cell[j].s8;
-          if (WJ) lnJ[j] = cl;
-          if (WY) lnY[j] = cl || near;  // Y0 is singular at 0
-          // B is needed where an adjacent interval takes the closed form
-          const bool nb = WY ? (lcY || lnY[j]) : (lcJ || lnJ[j]);
-          cell[j].template eval_scaled<WJ, WY>(r, (T)gm.z, (T)gm.w, nb, Jz, Yz);
-          const T u0 = fjs::fmaT(-cell[j].k2, q0.C, q0.A);
-          const T u1 = MT::NIN > 1 ? fjs::fmaT(-cell[j].k2, q1.C, q1.A) : T(0);
-          accumulate_station<MODE, T>(acc0[j], u0, u1, WJ ? Jz.z0 : T(0), WY ? Yz.z0 : T(0));
-          accumulate_station<MODE, T>(acc1[j], q0.B, q1.B, WJ ? Jz.z1 : T(0), WY ? Yz.z1 : T(0));
-          const bool exJ = WJ && (lcJ || !fold_cur), exY = WY && (lcY || !fold_cur);
-          if (exJ || exY) {
-            // interval (i-1, i) (never at i = 0)
-            const float4 gp = __ldg(a.geo + i - 1);
-            ZB<T> pJ{}, pY{};
-            if constexpr (kCarry) {
-              pJ = zpJ[j];
-              pY = zpY[j];
-            } else {
-              cell[j].template eval_scaled<WJ, WY>((T)gp.x, (T)gp.z, (T)gp.w, lcJ || lcY, pJ, pY);
-            }
-            const T gA0 = __ldg(&q0p[qi - a.nf].g);
-            const T gA1 = MT::NIN > 1 ? __ldg(&q1p[qi - a.nf].g) : T(0);
-            const Acc2<T> e = explicit_interval<MODE, T>(cell[j], exJ, exY, lcJ, lcY, fold_cur,
-                                                         (T)gp.y, (T)gp.x, (T)gp.w, r, (T)gm.w, pJ,
-                                                         Jz, pY, Yz, gA0, q0.g, gA1, q1.g);
-            acc0[j][0] += e.v[0];
-            acc0[j][1] += e.v[1];
-          }
-          if constexpr (kCarry) {
-            if (WJ) zpJ[j] = Jz;
-            if (WY) zpY[j] = Yz;
-          }
-        }
+      // smallest r of the chunk (the input need not be sorted): at or above
+      // s8w every station of the chunk has x >= 8 in every cell of the warp
+      float rmin = INFINITY;
+      for (int t = i0 + lane; t < i1; t += 32) rmin = fminf(rmin, __ldg(a.rs + t));
+      for (int o = 16; o > 0; o >>= 1) rmin = fminf(rmin, __shfl_xor_sync(0xffffffffu, rmin, o));
+      if ((T)rmin >= s8w) {
+        CCFJ_PRAGMA(unroll CCFJ_STATION_UNROLL)
+        for (int i = i0; i < i1; ++i) station(BoolTag<true>{}, i);
+      } else {
+        CCFJ_PRAGMA(unroll CCFJ_STATION_UNROLL)
+        for (int i = i0; i < i1; ++i) station(BoolTag<false>{}, i);
       }
 #pragma unroll
       for (int j = 0; j < CPT; ++j) {
@@ -605,7 +665,7 @@ __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
       res[1] = gam * tot[j][1];
       // k = 0 (f = 0) divides by zero in the reference: NaN
       const float v = cell[j].k == T(0) ? __int_as_float(0x7fffffff) : finish<MODE, T>(res, T(1));
-      if (c0 + j < a.nc) a.out[(long long)(c0 + j) * a.nf + fi] = v;
+      if (f_valid && c0 + j < a.nc) a.out[(long long)(c0 + j) * a.nf + fi] = v;
     }
   } else {
     for (int i0 = 0; i0 < a.nr; i0 += kChunk) {
@@ -633,7 +693,7 @@ __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
     }
 #pragma unroll
     for (int j = 0; j < CPT; ++j)
-      if (c0 + j < a.nc) a.out[(long long)(c0 + j) * a.nf + fi] = finish<MODE, T>(tot[j], T(1));
+      if (f_valid && c0 + j < a.nc) a.out[(long long)(c0 + j) * a.nf + fi] = finish<MODE, T>(tot[j], T(1));
   }
 }
 

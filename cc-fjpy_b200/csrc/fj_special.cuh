@@ -69,9 +69,15 @@ FJ_HD float rcp_fast(float x) {
   return 1.0f / x;
 #endif
 }
+// The SFU approximations below use their flush-to-zero forms: arguments and
+// results here are never subnormal in any way that matters (a subnormal
+// sine argument is 0 to within 1e-38), and the forms need no subnormal
+// fix-up instructions.
 FJ_HD float rsqrt_fast(float x) {
 #ifdef __CUDA_ARCH__
-  return rsqrtf(x);
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
 #else
   return 1.0f / sqrtf(x);
 #endif
@@ -80,7 +86,7 @@ FJ_HD float rsqrt_fast(float x) {
 FJ_HD float sqrt_fast(float x) {
 #ifdef __CUDA_ARCH__
   float y;
-  asm("sqrt.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
   return y;
 #else
   return sqrtf(x);
@@ -150,7 +156,9 @@ FJ_HD float chi_cycles_f32(float p_hi, float p_lo) {
 // host build (used by the CPU tests of the polynomials) uses libm.
 FJ_HD void sincos_cycles_f32(float u, float& s, float& c) {
 #ifdef __CUDA_ARCH__
-  __sincosf(kTwoPiF * u, &s, &c);
+  const float a = kTwoPiF * u;
+  asm("sin.approx.ftz.f32 %0, %1;" : "=f"(s) : "f"(a));
+  asm("cos.approx.ftz.f32 %0, %1;" : "=f"(c) : "f"(a));
 #else
   const double a = kTwoPi * (double)u;
   s = (float)sin(a);

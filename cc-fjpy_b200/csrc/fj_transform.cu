@@ -246,8 +246,10 @@ long long tune_key(const ccfj_fj_args& a) {
 // two-input Bessel form and the trapezoid, one for the two-basis forms
 // (their register use leaves too few warps resident with more).
 int default_cpt_for(int mode, int itype) {
-  (void)mode;  // under the 64-register cap 2 velocities win (or tie) in every mode
-  return itype == 0 ? 4 : 2;
+  if (itype == 0) return 4;
+  // two-basis modes recompute station i-1 on their explicit intervals and
+  // share the per-station loads best over 4 velocities
+  return (mode == CCFJ_MODE_J_MINUS_Y || mode == CCFJ_MODE_ABS_H) ? 4 : 2;
 }
 
 int tuned_cpt(const ccfj_fj_args& a) {
