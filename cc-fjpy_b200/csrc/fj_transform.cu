@@ -21,6 +21,7 @@
 // coalesced rows and r / dr are warp-uniform broadcasts.
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 #include <map>
 #include <mutex>
 #include <vector>
@@ -455,8 +456,195 @@ static int validate(const ccfj_fj_args* a) {
   return CCFJ_OK;
 }
 
+// ------------------------------------------ host memory, in frequency blocks
+// Frequency columns are independent (the per-frequency normalisation
+// included), so a large host-memory transform without the Hilbert transform
+// (which needs whole rows) runs in column blocks. The host gathers block
+// p+1's columns into one of two pinned staging buffers while the upload (one
+// contiguous DMA) and the transform of block p run on the GPU. Blocks
+// alternate between two library-owned streams so that one block's last wave
+// overlaps the next block's first; all downloads are issued after the last
+// upload (a pageable download would otherwise hold the host until its block
+// finished, and the next gather with it). The staging buffers (2 x 64 MiB of
+// pinned host memory per device) are allocated on first use and kept.
+namespace {
+constexpr int kHostMaxDevices = 64;
+constexpr size_t kStageBytes = size_t(64) << 20;
+constexpr int kMaxHostBlocks = 32;
+std::mutex g_host_mu;
+struct HostPipe {
+  cudaStream_t st[2] = {nullptr, nullptr};
+  void* stage[2] = {nullptr, nullptr};
+  cudaEvent_t staged[2] = {nullptr, nullptr};  // the upload from stage[k] has finished
+  std::mutex use;  // one blocked transform at a time uses the staging buffers
+};
+HostPipe g_host_pipe[kHostMaxDevices];
+
+int host_pipe(HostPipe** out) {
+  int dev = 0;
+  CCFJ_CUDA_TRY(cudaGetDevice(&dev));
+  CCFJ_REQUIRE(dev >= 0 && dev < kHostMaxDevices, "ccfj_fj_v1: device ordinal %d", dev);
+  std::lock_guard<std::mutex> lk(g_host_mu);
+  HostPipe& hp = g_host_pipe[dev];
+  for (int k = 0; k < 2; ++k) {
+    if (!hp.st[k]) CCFJ_CUDA_TRY(cudaStreamCreateWithFlags(&hp.st[k], cudaStreamNonBlocking));
+    if (!hp.stage[k]) CCFJ_CUDA_TRY(cudaHostAlloc(&hp.stage[k], kStageBytes, cudaHostAllocDefault));
+    if (!hp.staged[k])
+      CCFJ_CUDA_TRY(cudaEventCreateWithFlags(&hp.staged[k], cudaEventDisableTiming));
+  }
+  *out = &hp;
+  return CCFJ_OK;
+}
+
+// Blocks worth splitting into: about 40 MB of spectra each (each must fit a
+// staging buffer), at least 128 frequencies each.
+int host_block_count(const ccfj_fj_args& a, long long span_floats) {
+  if (a.hilbert) return 1;
+  const long long bytes = 4 * span_floats;
+  int n = (int)std::min<long long>(kMaxHostBlocks, (bytes + (40ll << 20) - 1) / (40ll << 20));
+  n = std::min(n, a.nf / 128);
+  // a block of nf/n frequencies spans about bytes/n (plus one column): keep
+  // that within a staging buffer
+  if (n >= 2 && bytes / n + bytes / a.nf * 2 > (long long)kStageBytes) return 1;
+  return std::max(n, 1);
+}
+}  // namespace
+
+static int fj_host_blocks(const ccfj_fj_args& a, cudaStream_t s, int nblk, int nin, bool merged) {
+  HostPipe* hp = nullptr;
+  int st = host_pipe(&hp);
+  if (st != CCFJ_OK) return st;
+  // one call at a time per device uses the staging buffers
+  std::lock_guard<std::mutex> pipe_lock(hp->use);
+  cudaStream_t hs[2] = {hp->st[0], hp->st[1]};
+  Scratch sc(s);
+  float* dr = sc.get_n<float>(a.nr);
+  float* df = sc.get_n<float>(a.nf);
+  float* dc = sc.get_n<float>(a.nc);
+  long long* dp = a.perm ? sc.get_n<long long>(a.nr) : nullptr;
+  if (!dr || !df || !dc || (a.perm && !dp)) return CCFJ_ERR_ALLOC;
+  CCFJ_CUDA_TRY(cudaMemcpyAsync(dr, a.r, sizeof(float) * a.nr, cudaMemcpyHostToDevice, s));
+  CCFJ_CUDA_TRY(cudaMemcpyAsync(df, a.f, sizeof(float) * a.nf, cudaMemcpyHostToDevice, s));
+  CCFJ_CUDA_TRY(cudaMemcpyAsync(dc, a.c, sizeof(float) * a.nc, cudaMemcpyHostToDevice, s));
+  if (dp)
+    CCFJ_CUDA_TRY(cudaMemcpyAsync(dp, a.perm, sizeof(long long) * a.nr, cudaMemcpyHostToDevice, s));
+  // The regions one block copies: every input's columns of the block over
+  // all rows, as one region when the inputs interleave (Re / Im).
+  const int nreg = merged ? 1 : nin;
+  const float* reg_base[2] = {a.u[0], a.u[1]};
+  long long reg_extra = 0;  // floats between the first and the last input of a merged region
+  if (merged && nin == 2) {
+    reg_base[0] = std::min(a.u[0], a.u[1]);
+    reg_extra = std::max(a.u[0], a.u[1]) - reg_base[0];
+  }
+  struct Block {
+    int b0, b1;
+    long long width;  // floats per row of the block's device copy
+    float* du[2];
+    float* dout;
+  };
+  Block blk[kMaxHostBlocks];
+  for (int p = 0; p < nblk; ++p) {
+    Block& B = blk[p];
+    // boundaries on whole warps of 32 frequencies (blocks hold >= 128)
+    B.b0 = p == 0 ? 0 : (int)(((long long)a.nf * p / nblk) & ~31ll);
+    B.b1 = p == nblk - 1 ? a.nf : (int)(((long long)a.nf * (p + 1) / nblk) & ~31ll);
+    const long long c_lo = (long long)(a.col_begin + B.b0) * a.fstride * a.u_es;
+    const long long c_hi = (long long)(a.col_begin + B.b1 - 1) * a.fstride * a.u_es;
+    B.width = c_hi - c_lo + 1 + reg_extra;
+    if ((size_t)nreg * B.width * a.u_rows * sizeof(float) > kStageBytes)
+      return set_error(CCFJ_ERR_UNSUPPORTED, "ccfj_fj_v1: host block exceeds the staging buffer");
+    // the block's regions are contiguous on the device (one DMA)
+    B.du[0] = sc.get_n<float>((size_t)nreg * B.width * a.u_rows);
+    if (!B.du[0]) return CCFJ_ERR_ALLOC;
+    B.du[1] = B.du[0] + (size_t)B.width * a.u_rows;
+    B.dout = sc.get_n<float>((size_t)a.nc * (B.b1 - B.b0));
+    if (!B.dout) return CCFJ_ERR_ALLOC;
+  }
+  cudaEvent_t ready = nullptr, done[2] = {nullptr, nullptr};
+  CCFJ_CUDA_TRY(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+  for (int k = 0; k < 2; ++k) CCFJ_CUDA_TRY(cudaEventCreateWithFlags(&done[k], cudaEventDisableTiming));
+  auto destroy = [&]() {
+    cudaEventDestroy(ready);
+    for (int k = 0; k < 2; ++k) cudaEventDestroy(done[k]);
+  };
+  auto fail = [&](int status) {
+    // leave no work of this call running on the library's streams
+    for (int k = 0; k < 2; ++k) cudaStreamSynchronize(hs[k]);
+    destroy();
+    return status;
+  };
+  if (cudaEventRecord(ready, s) != cudaSuccess)
+    return fail(set_error(CCFJ_ERR_CUDA, "ccfj_fj_v1: cudaEventRecord failed"));
+  for (int k = 0; k < 2; ++k)
+    if (cudaStreamWaitEvent(hs[k], ready, 0) != cudaSuccess)
+      return fail(set_error(CCFJ_ERR_CUDA, "ccfj_fj_v1: cudaStreamWaitEvent failed"));
+  for (int p = 0; p < nblk; ++p) {
+    Block& B = blk[p];
+    cudaStream_t cs = hs[p & 1];
+    const long long c_lo = (long long)(a.col_begin + B.b0) * a.fstride * a.u_es;
+    // gather the block's columns into staging buffer p % 2 once its previous
+    // upload has finished, then upload it in one piece
+    const int k = p & 1;
+    cudaError_t e = cudaEventSynchronize(hp->staged[k]);
+    if (e != cudaSuccess)
+      return fail(set_error(CCFJ_ERR_CUDA, "ccfj_fj_v1: staging wait failed: %s",
+                            cudaGetErrorString(e)));
+    float* stg = static_cast<float*>(hp->stage[k]);
+    const size_t row_bytes = B.width * sizeof(float);
+    for (int g = 0; g < nreg; ++g) {
+      const float* src = reg_base[g] + c_lo;
+      float* dst = stg + (size_t)g * B.width * a.u_rows;
+      for (long long row = 0; row < a.u_rows; ++row)
+        memcpy(dst + row * B.width, src + row * a.u_ld, row_bytes);
+    }
+    e = cudaMemcpyAsync(B.du[0], stg, (size_t)nreg * row_bytes * a.u_rows, cudaMemcpyHostToDevice,
+                        cs);
+    if (e == cudaSuccess) e = cudaEventRecord(hp->staged[k], cs);
+    if (e != cudaSuccess)
+      return fail(set_error(CCFJ_ERR_CUDA, "ccfj_fj_v1: block upload failed: %s",
+                            cudaGetErrorString(e)));
+    ccfj_fj_args d = a;
+    d.device_ptrs = 1;
+    for (int j = 0; j < nin; ++j)
+      d.u[j] = merged ? B.du[0] + (a.u[j] - reg_base[0]) : B.du[j];
+    d.u_ld = B.width;
+    d.col_begin = 0;
+    d.nf = B.b1 - B.b0;
+    d.nf_total = d.nf;
+    d.u_ncols = (d.nf - 1) * a.fstride + 1;
+    d.r = dr;
+    d.f = df + B.b0;
+    d.c = dc;
+    d.perm = dp;
+    d.out = B.dout;
+    st = fj_device(d, cs);
+    if (st != CCFJ_OK) return fail(st);
+  }
+  for (int p = 0; p < nblk; ++p) {
+    const Block& B = blk[p];
+    const int w = B.b1 - B.b0;
+    const cudaError_t e = cudaMemcpy2DAsync(a.out + B.b0, a.nf * sizeof(float), B.dout,
+                                            w * sizeof(float), w * sizeof(float), a.nc,
+                                            cudaMemcpyDeviceToHost, hs[p & 1]);
+    if (e != cudaSuccess)
+      return fail(set_error(CCFJ_ERR_CUDA, "ccfj_fj_v1: block download failed: %s",
+                            cudaGetErrorString(e)));
+  }
+  // the scratch is freed on s: s waits for both streams
+  for (int k = 0; k < 2; ++k) {
+    if (cudaEventRecord(done[k], hs[k]) != cudaSuccess || cudaStreamWaitEvent(s, done[k], 0) != cudaSuccess)
+      return fail(set_error(CCFJ_ERR_CUDA, "ccfj_fj_v1: stream join failed"));
+  }
+  const cudaError_t e = cudaStreamSynchronize(s);
+  destroy();
+  if (e != cudaSuccess)
+    return set_error(CCFJ_ERR_CUDA, "ccfj_fj_v1: %s", cudaGetErrorString(e));
+  return CCFJ_OK;
+}
+
 // Host-memory variant: copies the inputs in, runs the device path, copies
-// out back and waits.
+// out back and waits (in frequency blocks when that pays, see above).
 static int fj_host(const ccfj_fj_args& a, cudaStream_t s) {
   const int nin = a.hilbert ? 1 : nin_of(a.mode);
   const long long rows = a.u_rows;
@@ -479,6 +667,8 @@ static int fj_host(const ccfj_fj_args& a, cudaStream_t s) {
       merged = true;
     }
   }
+  const int nblk = host_block_count(a, merged ? (long long)(hi - lo) : nin * span);
+  if (nblk > 1) return fj_host_blocks(a, s, nblk, nin, merged);
   Scratch sc(s);
   ccfj_fj_args d = a;
   d.device_ptrs = 1;

@@ -204,3 +204,57 @@ def test_frequency_window_equals_full_transform(ccfj, func, itype):
     for a, b in ((0, 7), (7, 13), (13, nf), (3, 4)):
         part = dist._cuda_columns(*args, (a, b))
         assert np.array_equal(part, full[:, a:b], equal_nan=True)
+
+
+@pytest.mark.parametrize("mode,merged", [(0, True), (3, True), (3, False)])
+def test_host_blocks_equal_device_path(ccfj, lib, mode, merged):
+    """A host-memory transform large enough to run in frequency blocks (the
+    upload of one block overlapping the transform of the previous one)
+    gives the same bits as the same transform on device-resident inputs."""
+    import torch
+    from ccfj import _lib
+    rng = np.random.default_rng(41)
+    nr, nf, nc = 2600, 4096, 24
+    r = np.sort(rng.uniform(1e3, 3e5, nr)).astype(np.float32)
+    f = np.linspace(0.01, 1.5, nf).astype(np.float32)
+    c = np.linspace(800.0, 4500.0, nc).astype(np.float32)
+    uf = (rng.standard_normal((nr, nf)) + 1j * rng.standard_normal((nr, nf))).astype(np.complex64)
+    perm = rng.permutation(nr).astype(np.int64)
+    flat = uf.view(np.float32)                       # (nr, 2 nf): Re, Im interleaved
+    if merged:
+        ins = [flat, flat[:, 1:]]                    # one region, Re and Im
+        ld, es = 2 * nf, 2
+    else:
+        ins = [np.ascontiguousarray(flat[:, 0::2]), np.ascontiguousarray(flat[:, 1::2])]
+        ld, es = nf, 1
+
+    def args(us, rp, fp, cp, pp, outp, device):
+        a = _lib.FjArgs()
+        a.struct_size = ctypes.sizeof(a)
+        a.nr, a.nf, a.nc = nr, nf, nc
+        a.itype, a.mode, a.precision, a.normalize, a.device_ptrs = 1, mode, 0, 1, int(device)
+        a.u[0] = us[0]
+        a.u[1] = us[1] if mode == 3 else None
+        a.u_ld, a.u_rows, a.u_es, a.u_ncols, a.fstride = ld, nr, es, nf, 1
+        a.perm, a.r, a.f, a.c, a.out = pp, rp, fp, cp, outp
+        return a
+
+    out_h = np.empty((nc, nf), dtype=np.float32)
+    a = args([x.ctypes.data for x in ins], r.ctypes.data, f.ctypes.data, c.ctypes.data,
+             perm.ctypes.data, out_h.ctypes.data, False)
+    _lib.check(lib.ccfj_fj_v1(ctypes.byref(a), None))
+    T = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda()
+         for k, v in dict(r=r, f=f, c=c, perm=perm).items()}
+    if merged:
+        dflat = torch.from_numpy(flat).cuda()
+        us = [dflat.data_ptr(), dflat.data_ptr() + 4]
+        keep = [dflat]
+    else:
+        keep = [torch.from_numpy(x).cuda() for x in ins]
+        us = [t.data_ptr() for t in keep]
+    out_d = torch.empty((nc, nf), device="cuda")
+    a = args(us, T["r"].data_ptr(), T["f"].data_ptr(), T["c"].data_ptr(), T["perm"].data_ptr(),
+             out_d.data_ptr(), True)
+    _lib.check(lib.ccfj_fj_v1(ctypes.byref(a), None))
+    torch.cuda.synchronize()
+    assert np.array_equal(out_h, out_d.cpu().numpy(), equal_nan=True)
