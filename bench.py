@@ -413,9 +413,20 @@ def _time_device(fn, steps, warmup):
     return e0.elapsed_time(e1) / 1e3 / steps
 
 
+def _max_err(y32, y64, sample):
+    e = np.abs(y32.astype(np.float64) - y64.astype(np.float64))
+    return {"max_abs_err_vs_fp64_normalised": float(np.nanmax(e)),
+            "nan_positions_equal": bool(np.array_equal(np.isnan(y32), np.isnan(y64))),
+            "sample": sample}
+
+
 def run_config(args):
-    """Device-resident timing of SURVEY configs 1, 3, 4 and 5 (one JSON line
-    each; the headline bench line is config 2)."""
+    """Device-resident timing of the other workloads (one JSON line each; the
+    headline bench line is the large-array noise workload, 2):
+      1  small noise array: 200 pairs x 512 f x 300 c
+      3  fj_earthquake: 500 traces x 8192 samples, rFFT on the GPU, nf 1024, 800 c
+      4  MWFJ: 1000 traces x 16384 samples, 64 windows, nf 1024, 2000 c
+      5  ragged batch: 512 subarrays (50-20000 pairs each), nf 1024, 500 c"""
     import torch
     import cases
     from ccfj import _lib, _batch, _eq
@@ -437,8 +448,12 @@ def run_config(args):
                       d["f"], d["c"], out)
         t = _time_device(lambda: _lib.check(lib.ccfj_fj_v1(ctypes.byref(a), sp)), args.steps,
                          args.warmup)
+        y32 = out.cpu().numpy()
+        a.precision = _lib.PREC_FP64
+        _lib.check(lib.ccfj_fj_v1(ctypes.byref(a), sp))
         res.update(workload="fj_noise itype=1 func=0, 200 pairs x 512 f x 300 c", seconds=t,
-                   value=200 * 512 * 300 / t)
+                   value=200 * 512 * 300 / t,
+                   accuracy=_max_err(y32, out.cpu().numpy(), "all 300 x 512"))
     elif cfg in (3, 4):
         if cfg == 3:
             rng = np.random.default_rng(3)
@@ -481,6 +496,17 @@ def run_config(args):
         fn = lambda: _lib.check(lib.ccfj_fj_earthquake_v1(ctypes.byref(a), sp))  # noqa: E731
         t = _time_device(fn, max(1, args.steps // (4 if cfg == 4 else 1)), 1)
         terms = nw * nf * nc * ntr
+        # FP64 station-amortised form on the same spectra (MWFJ: its first 4
+        # windows, one transform per window)
+        y32 = out.cpu().numpy()
+        n64 = min(nw, 4)
+        a.precision = _lib.PREC_FP64
+        if nwin:
+            a.nwin = n64
+        _lib.check(lib.ccfj_fj_earthquake_v1(ctypes.byref(a), sp))
+        y64 = out[:n64].cpu().numpy()
+        res["accuracy"] = _max_err(y32[:n64], y64, "windows 0-%d" % (n64 - 1) if nwin else
+                                   "all 800 x 1024")
         res.update(workload=("fj_earthquake itype=1 func=0 with device rFFT, 500 traces x 8192 "
                              "samples, nf=1024 bins, nc=800" if cfg == 3 else
                              "MWFJ itype=1 func=0, 1000 traces x 16384 samples, 64 windows, "
@@ -555,6 +581,25 @@ def run_config(args):
 
         t_sep = _time_device(separate, 1, 1)
         terms = total * nf * nc
+        # FP64 station-amortised form of 8 subarrays (the largest, the
+        # smallest and 6 in between) against the batch's FP32 output
+        with torch.cuda.stream(s_cap):
+            batch_step()
+        s_cap.synchronize()
+        y32 = out.cpu().numpy()
+        lib.ccfj_batch_graph_cache_clear()
+        picks = np.unique(np.argsort(counts)[np.linspace(0, nsets - 1, 8).astype(int)])
+        o64 = torch.empty((nc, nf), device="cuda")
+        errs = []
+        for b in picks:
+            a = single[b]
+            a.precision, a.out = _lib.PREC_FP64, o64.data_ptr()
+            _lib.check(lib.ccfj_fj_v1(ctypes.byref(a), sp))
+            torch.cuda.synchronize()
+            errs.append(_max_err(y32[b], o64.cpu().numpy(), "")["max_abs_err_vs_fp64_normalised"])
+        res["accuracy"] = {"max_abs_err_vs_fp64_normalised": float(np.nanmax(errs)),
+                           "sample": "subarrays with %s pairs" % ", ".join(str(int(counts[b]))
+                                                                          for b in picks)}
         res.update(workload="512 subarrays, %d pairs in total (log-uniform 50-20000 each), "
                             "nf=1024, nc=500, itype=1 func=0; one persistent graph-replayed "
                             "launch" % total, seconds=t_batch, value=terms / t_batch,
@@ -582,7 +627,8 @@ def main():
                          "extras) for ncu captures: 'noise' = the first 512 frequencies of the "
                          "workload; 'mwfj' = the MWFJ configuration with 8 windows and 256 bins")
     ap.add_argument("--config", type=int, default=0, choices=(0, 1, 3, 4, 5),
-                    help="time another SURVEY configuration (device-resident; one JSON line)")
+                    help="time another workload (device-resident; one JSON line): 1 small noise array, "
+                         "3 earthquake, 4 MWFJ, 5 ragged batch")
     args = ap.parse_args()
     if args.config:
         return run_config(args)

@@ -258,3 +258,26 @@ def test_host_blocks_equal_device_path(ccfj, lib, mode, merged):
     _lib.check(lib.ccfj_fj_v1(ctypes.byref(a), None))
     torch.cuda.synchronize()
     assert np.array_equal(out_h, out_d.cpu().numpy(), equal_nan=True)
+
+
+@pytest.mark.parametrize("func", [0, 1])
+@pytest.mark.parametrize("zero_pair", [False, True])
+def test_wide_velocity_range(ccfj, func, zero_pair):
+    """Velocities over two decades (100-10000 m/s) at up to 2 Hz: k dr spans
+    the Hermite rule, folded intervals with closed-form corrections and
+    intervals left out of the fold, in one transform. With zero_pair, one
+    pair sits at zero distance (the J basis is finite there; the Y basis of
+    func 1 is singular at r = 0 and left out of that case)."""
+    if zero_pair and func == 1:
+        pytest.skip("Y0 is singular at r = 0")
+    rng = np.random.default_rng(77)
+    r = np.sort(rng.uniform(50.0, 8e4, 90))
+    if zero_pair:
+        r[0] = 0.0
+    f = np.linspace(0.02, 2.0, 36)
+    c = np.geomspace(100.0, 1e4, 70)
+    uf = cases.noise_spectra(rng, r, f, sigma=0.2, overtone=True)
+    y = _quiet(ccfj.fj_noise, uf, r, c, f, itype=1, func=func)
+    y64 = _quiet(O.fj_noise, uf, r, c, f, itype=1, func=func)
+    assert np.array_equal(np.isnan(y), np.isnan(y64))
+    assert O.rel_error(y, y64) <= TOL
