@@ -538,6 +538,30 @@ struct BoolTag {
   static constexpr bool value = B;
 };
 
+// Threads per CTA of the kernels built on fj_cells: 32 frequencies x 8
+// velocity rows.
+constexpr int kCellThreads = 256;
+
+// Shared-memory stage of the FP32 itype-1 loop: per buffer, the station
+// coefficients of a chunk for the CTA's 32 frequencies, and its geometry.
+// 33 KB (one input, 32 stations) or 32.5 KB (two inputs, 16 stations).
+template <int NIN>
+struct StageBuf {
+  static constexpr int kStations = NIN > 1 ? 16 : 32;
+  float4 coef[2][NIN][kStations][32];
+  float4 geo[2][kStations];
+};
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
 // CPT cells (f, c), (f, c + 1), ... per thread share the per-station loads.
 // The transform of the CPT cells (fi, c0), (fi, c0 + 1), ... of one data
 // set; shared by the grid kernel below and the persistent batch kernel.
@@ -547,9 +571,15 @@ __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
   constexpr bool WJ = MT::WJ, WY = MT::WY;
   // c0 is uniform across a warp (its lanes are 32 frequencies); lanes past
   // the last frequency compute the last one and store nothing, so that all
-  // 32 lanes stay active for the warp-wide steps below
-  if (c0 >= a.nc) return;
+  // 32 lanes stay active for the warp-wide steps below. The staged FP32
+  // itype-1 loop has CTA-wide barriers: a warp past the last velocity stays
+  // and helps with the staging.
+  constexpr bool kStaged = ITYPE == 1 && sizeof(T) == 4;
+  const bool c_valid = c0 < a.nc;
+  if (!kStaged && !c_valid) return;
+  c0 = c_valid ? c0 : 0;
   const bool f_valid = fi < a.nf;
+  const int fbase = fi - (int)(threadIdx.x & 31);  // first frequency of the warp (and CTA)
   fi = f_valid ? fi : a.nf - 1;
   Cell<T> cell[CPT];
   const float fl = a.f[fi];
@@ -583,14 +613,11 @@ __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
     T acc0[CPT][2], acc1[CPT][2];
     // One station: out += gam (y0 (A - k^2 C) - k y1 B), plus the explicit
     // interval (i-1, i) where it is not (only) in the folded sum.
-    auto station = [&](auto large_tag, int i) {
+    auto station = [&](auto large_tag, int i, const float4 gm, const StationCoef<T> q0,
+                       const StationCoef<T> q1) {
       constexpr bool LARGE = decltype(large_tag)::value;
-      const float4 gm = __ldg(a.geo + i);
       const T r = gm.x, D_next = gm.y;
       const long long qi = (long long)i * a.nf;
-      const StationCoef<T> q0 = load_coef(q0p + qi);
-      StationCoef<T> q1{};
-      if (MT::NIN > 1) q1 = load_coef(q1p + qi);
       const T dl8 = fabs(D) * d8;
 #pragma unroll
       for (int j = 0; j < CPT; ++j) {
@@ -635,28 +662,100 @@ __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
       D = D_next;
     };
     const int lane = threadIdx.x & 31;
-    for (int i0 = 0; i0 < a.nr; i0 += kChunk) {
-      const int i1 = min(a.nr, i0 + kChunk);
-#pragma unroll
-      for (int j = 0; j < CPT; ++j) acc0[j][0] = acc0[j][1] = acc1[j][0] = acc1[j][1] = T(0);
-      // smallest r of the chunk (the input need not be sorted): at or above
-      // s8w every station of the chunk has x >= 8 in every cell of the warp
-      float rmin = INFINITY;
-      for (int t = i0 + lane; t < i1; t += 32) rmin = fminf(rmin, __ldg(a.rs + t));
-      for (int o = 16; o > 0; o >>= 1) rmin = fminf(rmin, __shfl_xor_sync(0xffffffffu, rmin, o));
-      if ((T)rmin >= s8w) {
-        CCFJ_PRAGMA(unroll CCFJ_STATION_UNROLL)
-        for (int i = i0; i < i1; ++i) station(BoolTag<true>{}, i);
-      } else {
-        CCFJ_PRAGMA(unroll CCFJ_STATION_UNROLL)
-        for (int i = i0; i < i1; ++i) station(BoolTag<false>{}, i);
-      }
+    // Closes a chunk of stations: folds its partial sums into the totals.
+    auto flush = [&]() {
 #pragma unroll
       for (int j = 0; j < CPT; ++j) {
         tot[j][0] += fjs::fmaT(-cell[j].k, acc1[j][0], acc0[j][0]);
         tot[j][1] += fjs::fmaT(-cell[j].k, acc1[j][1], acc0[j][1]);
+        acc0[j][0] = acc0[j][1] = acc1[j][0] = acc1[j][1] = T(0);
+      }
+    };
+#pragma unroll
+    for (int j = 0; j < CPT; ++j) acc0[j][0] = acc0[j][1] = acc1[j][0] = acc1[j][1] = T(0);
+    if constexpr (kStaged) {
+      // The CTA's 8 warps share the 32 frequencies of fbase..fbase+31, so
+      // one copy of a chunk's station data in shared memory serves them all:
+      // chunks of S stations (coefficients and geometry) are staged with
+      // cp.async, double-buffered, while the previous chunk is computed.
+      using SB = StageBuf<MT::NIN>;
+      constexpr int S = SB::kStations;
+      __shared__ SB sb;
+      const int tid = threadIdx.y * 32 + threadIdx.x;
+      const StationCoef<float>* g0 = static_cast<const StationCoef<float>*>(a.gb[0]);
+      const StationCoef<float>* g1 = static_cast<const StationCoef<float>*>(a.gb[MT::NIN > 1 ? 1 : 0]);
+      auto stage = [&](int ch, int buf) {
+        const int i0 = ch * S;
+        const int n = min(S, a.nr - i0);
+        for (int t = tid; t < n * 32; t += kCellThreads) {
+          const int st = t >> 5;
+          const long long src = (long long)(i0 + st) * a.nf + min(fbase + (t & 31), a.nf - 1);
+          cp_async16(&sb.coef[buf][0][st][t & 31], g0 + src);
+          if (MT::NIN > 1) cp_async16(&sb.coef[buf][MT::NIN > 1 ? 1 : 0][st][t & 31], g1 + src);
+        }
+        for (int t = tid; t < n; t += kCellThreads) cp_async16(&sb.geo[buf][t], a.geo + i0 + t);
+        cp_async_commit();
+      };
+      const int nch = (a.nr + S - 1) / S;
+      stage(0, 0);
+      for (int ch = 0; ch < nch; ++ch) {
+        const int buf = ch & 1;
+        if (ch + 1 < nch)
+          stage(ch + 1, buf ^ 1);
+        else
+          cp_async_commit();  // one group per iteration keeps the count below
+        cp_async_wait<1>();   // this thread's copies of chunk ch have landed
+        __syncthreads();      // ... and everybody else's
+        const int i0 = ch * S;
+        const int n = min(S, a.nr - i0);
+        if (c_valid) {
+          // smallest r of the chunk (the input need not be sorted): at or
+          // above s8w every station of the chunk has x >= 8 in every cell of
+          // the warp
+          float rmin = lane < n ? sb.geo[buf][lane].x : INFINITY;
+          for (int o = 16; o > 0; o >>= 1)
+            rmin = fminf(rmin, __shfl_xor_sync(0xffffffffu, rmin, o));
+          auto run = [&](auto large_tag) {
+            CCFJ_PRAGMA(unroll CCFJ_STATION_UNROLL)
+            for (int st = 0; st < n; ++st) {
+              const float4 c0v = sb.coef[buf][0][st][lane];
+              float4 c1v = c0v;
+              if (MT::NIN > 1) c1v = sb.coef[buf][MT::NIN > 1 ? 1 : 0][st][lane];
+              station(large_tag, i0 + st, sb.geo[buf][st], StationCoef<T>{c0v.x, c0v.y, c0v.z, c0v.w},
+                      StationCoef<T>{c1v.x, c1v.y, c1v.z, c1v.w});
+            }
+          };
+          if ((T)rmin >= s8w)
+            run(BoolTag<true>{});
+          else
+            run(BoolTag<false>{});
+          flush();
+        }
+        __syncthreads();  // buffer buf is refilled by the stage() of the next iteration
+      }
+    } else {
+      for (int i0 = 0; i0 < a.nr; i0 += kChunk) {
+        const int i1 = min(a.nr, i0 + kChunk);
+        float rmin = INFINITY;
+        for (int t = i0 + lane; t < i1; t += 32) rmin = fminf(rmin, __ldg(a.rs + t));
+        for (int o = 16; o > 0; o >>= 1) rmin = fminf(rmin, __shfl_xor_sync(0xffffffffu, rmin, o));
+        auto run = [&](auto large_tag) {
+          for (int i = i0; i < i1; ++i) {
+            const long long qi = (long long)i * a.nf;
+            const StationCoef<T> q0 = load_coef(q0p + qi);
+            StationCoef<T> q1{};
+            if (MT::NIN > 1) q1 = load_coef(q1p + qi);
+            station(large_tag, i, __ldg(a.geo + i), q0, q1);
+          }
+        };
+        if ((T)rmin >= s8w)
+          run(BoolTag<true>{});
+        else
+          run(BoolTag<false>{});
+        flush();
       }
     }
+    if (!c_valid) return;
 #pragma unroll
     for (int j = 0; j < CPT; ++j) {
       const T gam = cell[j].gamma();

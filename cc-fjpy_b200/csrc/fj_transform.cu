@@ -248,9 +248,8 @@ long long tune_key(const ccfj_fj_args& a) {
 // (their register use leaves too few warps resident with more).
 int default_cpt_for(int mode, int itype) {
   if (itype == 0) return 4;
-  // two-basis modes recompute station i-1 on their explicit intervals and
-  // share the per-station loads best over 4 velocities
-  return (mode == CCFJ_MODE_J_MINUS_Y || mode == CCFJ_MODE_ABS_H) ? 4 : 2;
+  // two-basis modes hold twice the special-function state per velocity
+  return (mode == CCFJ_MODE_J_MINUS_Y || mode == CCFJ_MODE_ABS_H) ? 1 : 2;
 }
 
 int tuned_cpt(const ccfj_fj_args& a) {
