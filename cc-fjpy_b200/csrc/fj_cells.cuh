@@ -21,7 +21,7 @@ constexpr float kDefaultTau64 = 0.05f;
 constexpr int kChunk = 64;           // stations per partial sum
 // Unroll factor of the itype-1 station loop.
 #ifndef CCFJ_STATION_UNROLL
-#define CCFJ_STATION_UNROLL 1
+#define CCFJ_STATION_UNROLL 2
 #endif
 #define CCFJ_PRAGMA_(x) _Pragma(#x)
 #define CCFJ_PRAGMA(x) CCFJ_PRAGMA_(x)

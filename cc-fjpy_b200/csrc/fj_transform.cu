@@ -56,8 +56,10 @@ __global__ void fj_prep_geom_kernel(const float* __restrict__ rs, int nr, float*
 
 template <int MODE, int ITYPE, typename T, int CPT>
 __global__ void __launch_bounds__(256, fj_min_blocks<T>()) fj_amortized_kernel(FjDev a) {
-  fj_cells<MODE, ITYPE, T, CPT>(a, blockIdx.x * blockDim.x + threadIdx.x,
-                                (blockIdx.y * blockDim.y + threadIdx.y) * CPT);
+  // velocity tiles on grid x: the CTAs of one frequency tile run side by
+  // side and share its station coefficients in L2
+  fj_cells<MODE, ITYPE, T, CPT>(a, blockIdx.y * blockDim.x + threadIdx.x,
+                                (blockIdx.x * blockDim.y + threadIdx.y) * CPT);
 }
 
 // ------------------------------------------ FP64 comparator (plain form)
@@ -183,7 +185,7 @@ int g_force_cpt = 0;
 template <int MODE, typename T, int CPT>
 void launch_amortized_cpt(int itype, const FjDev& d, cudaStream_t s) {
   const dim3 block(32, 8);
-  const dim3 grid(div_up(d.nf, 32), div_up(d.nc, 8 * CPT));
+  const dim3 grid(div_up(d.nc, 8 * CPT), div_up(d.nf, 32));
   if (itype == 1)
     fj_amortized_kernel<MODE, 1, T, CPT><<<grid, block, 0, s>>>(d);
   else
@@ -247,9 +249,8 @@ long long tune_key(const ccfj_fj_args& a) {
 // two-input Bessel form and the trapezoid, one for the two-basis forms
 // (their register use leaves too few warps resident with more).
 int default_cpt_for(int mode, int itype) {
-  if (itype == 0) return 4;
-  // two-basis modes hold twice the special-function state per velocity
-  return (mode == CCFJ_MODE_J_MINUS_Y || mode == CCFJ_MODE_ABS_H) ? 1 : 2;
+  (void)mode;  // with the stations staged in shared memory, 2 wins in every itype-1 mode
+  return itype == 0 ? 4 : 2;
 }
 
 int tuned_cpt(const ccfj_fj_args& a) {
@@ -425,6 +426,10 @@ static int validate(const ccfj_fj_args* a) {
                (int)sizeof(ccfj_fj_args));
   CCFJ_REQUIRE(a->nr >= 1 && a->nf >= 1 && a->nc >= 1, "ccfj_fj_v1: nr=%d nf=%d nc=%d must be >= 1",
                a->nr, a->nf, a->nc);
+  // frequency tiles of 32 and velocity rows of 8 are grid dimensions y
+  CCFJ_REQUIRE(a->nf <= 65535 * 32 && a->nc <= 65535 * 8,
+               "ccfj_fj_v1: nf=%d (max %d) or nc=%d (max %d) too large for one launch", a->nf,
+               65535 * 32, a->nc, 65535 * 8);
   CCFJ_REQUIRE(a->itype == 0 || a->itype == 1, "ccfj_fj_v1: itype must be 0 or 1 (got %d)",
                a->itype);
   CCFJ_REQUIRE(a->mode >= CCFJ_MODE_J && a->mode <= CCFJ_MODE_ABS_H, "ccfj_fj_v1: bad mode %d",

@@ -230,8 +230,8 @@ CCFJ_API int ccfj_self_test_wait_timeout(void *stream);
  * (device pointers; out is overwritten), records the fastest for the
  * problem's class (mode, itype and the powers of two of nr, nf, nc) for all
  * later calls of this process, and returns it. ccfj_set_fj_variant(cpt)
- * forces a variant (0 restores the tuned choice, or the default: 4 for
- * itype 0; for itype 1, 1 for MODE_J_MINUS_Y / MODE_ABS_H and 2 otherwise). */
+ * forces a variant (0 restores the tuned choice, or the default: 2 for
+ * itype 1, 4 for itype 0). */
 CCFJ_API int ccfj_autotune_fj_v1(const ccfj_fj_args *args, void *stream, int *best_cpt,
                                  float *best_ms);
 CCFJ_API int ccfj_set_fj_variant(int cpt);
