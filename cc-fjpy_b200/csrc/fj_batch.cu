@@ -158,8 +158,10 @@ __global__ void __launch_bounds__(256, fj_min_blocks<float>()) fj_batch_persiste
     a.gb[0] = static_cast<const char*>(bd.base.gb[0]) + o * a.nf * esz;
     if (ModeTraits<MODE>::NIN > 1) a.gb[1] = static_cast<const char*>(bd.base.gb[1]) + o * a.nf * esz;
     a.out += (long long)b * a.nc * a.nf;
-    const int fi = (rem % bd.ftiles) * 32 + threadIdx.x;
-    const int c0 = ((rem / bd.ftiles) * 8 + threadIdx.y) * CPT;
+    // velocity tiles fastest: the items of one frequency tile run side by
+    // side and share its station coefficients in L2
+    const int fi = (rem / bd.ctiles) * 32 + threadIdx.x;
+    const int c0 = ((rem % bd.ctiles) * 8 + threadIdx.y) * CPT;
     fj_cells<MODE, ITYPE, float, CPT>(a, fi, c0);
   }
 }

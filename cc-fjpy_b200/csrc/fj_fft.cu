@@ -15,6 +15,8 @@
 //
 // Output: complex [rows][nbins] as interleaved float pairs, row = sorted
 // trace i (times window w for MWFJ: row = w * ntr + i).
+#include <stdint.h>
+
 #include "ccfj_core.cuh"
 #include "fj_fft.cuh"
 
@@ -107,6 +109,179 @@ __global__ void __launch_bounds__(kFftThreads) rfft_pow2_kernel(FftJob job, cons
   }
 }
 
+// ------------------------------------------ Stockham FFT, 16 points per thread
+// For 512 <= M <= 8192 complex points (N = 2M real samples): M/16 threads per
+// row, each holding 16 points in registers. The passes follow Stockham's
+// autosort formulation (no bit reversal): a pass of radix R over sub-
+// transforms of size Ns reads in[j + r M/R] (r < R), multiplies by
+// e^{-2 pi i r (j mod Ns) / (Ns R)}, takes an R-point DFT and writes
+// out[(j / Ns) Ns R + (j mod Ns) + r Ns]. Radix 16 while at least 16 remain,
+// then one pass of the remaining radix (2, 4 or 8, each thread doing 16/R
+// butterflies): 4 passes for M = 8192 instead of 13 radix-2 stages. The
+// first pass reads the (tapered) trace straight from global memory; the
+// others go through one shared-memory buffer with a pad slot per 16
+// entries, so that the strided writes of the early passes do not collide
+// in the banks.
+constexpr int kStockMinM = 512, kStockMaxM = 8192;
+
+__device__ __forceinline__ int spad(int i) { return i + (i >> 4); }
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// In-register R-point DFT (R = 2, 4, 8, 16), natural order in and out:
+// radix-2 decimation in time over bit-reversed register indices, with the
+// 16th roots of unity as constants.
+template <int R>
+__device__ __forceinline__ void dft_pow2(float2* v) {
+  // cos and -sin of 2 pi m / 16, m = 0..7
+  constexpr float kC[8] = {1.0f, 0.92387953251128674f, 0.70710678118654752f,
+                           0.38268343236508977f, 0.0f, -0.38268343236508977f,
+                           -0.70710678118654752f, -0.92387953251128674f};
+  constexpr float kS[8] = {0.0f, -0.38268343236508977f, -0.70710678118654752f,
+                           -0.92387953251128674f, -1.0f, -0.92387953251128674f,
+                           -0.70710678118654752f, -0.38268343236508977f};
+  constexpr int LOG = R == 2 ? 1 : R == 4 ? 2 : R == 8 ? 3 : 4;
+  float2 t[R];
+#pragma unroll
+  for (int i = 0; i < R; ++i) {
+    int rev = 0;
+#pragma unroll
+    for (int b = 0; b < LOG; ++b) rev |= ((i >> b) & 1) << (LOG - 1 - b);
+    t[rev] = v[i];
+  }
+#pragma unroll
+  for (int h = 1; h < R; h *= 2) {
+#pragma unroll
+    for (int g = 0; g < R; g += 2 * h) {
+#pragma unroll
+      for (int jj = 0; jj < h; ++jj) {
+        const int m = jj * (8 / h);  // e^{-2 pi i jj / (2h)} = W16^m
+        const float2 w = make_float2(kC[m], kS[m]);
+        const float2 u = t[g + jj];
+        const float2 x = h == 1 ? t[g + jj + h] : cmul(t[g + jj + h], w);
+        t[g + jj] = make_float2(u.x + x.x, u.y + x.y);
+        t[g + jj + h] = make_float2(u.x - x.x, u.y - x.y);
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < R; ++i) v[i] = t[i];
+}
+
+// e^{-2 pi i t / M} for t < M from the half table tw (t < M/2).
+__device__ __forceinline__ float2 twiddle_full(const float2* __restrict__ tw, int t, int M) {
+  const int h = M >> 1;
+  const float2 w = __ldg(tw + (t < h ? t : t - h));
+  return t < h ? w : make_float2(-w.x, -w.y);
+}
+
+// One Stockham pass of radix R over the 16 registers of thread tid (16/R
+// butterflies j = tid + g P), writing the outputs to shared memory.
+template <int R>
+__device__ __forceinline__ void stockham_pass(float2 (&v)[16], float2* sz, int M, int Ns,
+                                              const float2* __restrict__ tw, int tid, int P) {
+#pragma unroll
+  for (int g = 0; g < 16 / R; ++g) {
+    const int j = tid + g * P;
+    const int k = j % Ns;
+    float2* u = v + g * R;
+    if (Ns > 1) {
+      const int step = k * (M / (Ns * R));
+#pragma unroll
+      for (int r = 1; r < R; ++r) u[r] = cmul(u[r], twiddle_full(tw, r * step, M));
+    }
+    dft_pow2<R>(u);
+    const int o = (j / Ns) * Ns * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) sz[spad(o + r * Ns)] = u[r];
+  }
+}
+
+// Reads the inputs of a radix-R pass from shared memory.
+template <int R>
+__device__ __forceinline__ void stockham_load(float2 (&v)[16], const float2* sz, int M, int tid,
+                                              int P) {
+#pragma unroll
+  for (int g = 0; g < 16 / R; ++g) {
+    const int j = tid + g * P;
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[g * R + r] = sz[spad(j + r * (M / R))];
+  }
+}
+
+__global__ void __launch_bounds__(kStockMaxM / 16, 2)
+    rfft_stockham_kernel(FftJob job, const float2* __restrict__ tw) {
+  extern __shared__ float2 sz[];
+  const int M = job.npts >> 1;
+  const int P = M >> 4;
+  const int tid = threadIdx.x;
+  const int row = blockIdx.x;
+  const int i = row % job.ntr;  // sorted trace
+  const long long src_row = job.perm ? job.perm[i] : i;
+  const float2* x = reinterpret_cast<const float2*>(job.u + src_row * job.u_ld);
+  const bool taper = job.taper != nullptr;
+  TaperSpec tp;
+  if (taper) tp = job.taper[row];
+  // first pass (radix 16, Ns = 1): z[m] = x[2m] + i x[2m+1], m = tid + r P
+  float2 v[16];
+#pragma unroll
+  for (int r = 0; r < 16; ++r) {
+    const int m = tid + r * P;
+    float2 z = __ldg(x + m);
+    if (taper) {
+      z.x *= taper_value(2 * m, tp);
+      z.y *= taper_value(2 * m + 1, tp);
+    }
+    v[r] = z;
+  }
+  stockham_pass<16>(v, sz, M, 1, tw, tid, P);
+  __syncthreads();
+  int Ns = 16;
+  while (Ns < M) {
+    const int rem = M / Ns;
+    if (rem >= 16) {
+      stockham_load<16>(v, sz, M, tid, P);
+      __syncthreads();
+      stockham_pass<16>(v, sz, M, Ns, tw, tid, P);
+      Ns *= 16;
+    } else if (rem == 8) {
+      stockham_load<8>(v, sz, M, tid, P);
+      __syncthreads();
+      stockham_pass<8>(v, sz, M, Ns, tw, tid, P);
+      Ns *= 8;
+    } else if (rem == 4) {
+      stockham_load<4>(v, sz, M, tid, P);
+      __syncthreads();
+      stockham_pass<4>(v, sz, M, Ns, tw, tid, P);
+      Ns *= 4;
+    } else {
+      stockham_load<2>(v, sz, M, tid, P);
+      __syncthreads();
+      stockham_pass<2>(v, sz, M, Ns, tw, tid, P);
+      Ns *= 2;
+    }
+    __syncthreads();
+  }
+  // real-transform split, bins k < nbins (k <= M)
+  float2* out = job.out + (long long)row * job.nbins;
+  for (int kk = tid; kk < job.nbins; kk += P) {
+    const int k = kk * job.bin_stride;
+    if (k > M) {
+      out[kk] = make_float2(0.f, 0.f);
+      continue;
+    }
+    const float2 zk = sz[spad(k == M ? 0 : k)];
+    const float2 zm = sz[spad(k == 0 ? 0 : M - k)];
+    const float er = 0.5f * (zk.x + zm.x), ei = 0.5f * (zk.y - zm.y);
+    const float orr = 0.5f * (zk.y + zm.y), oi = -0.5f * (zk.x - zm.x);
+    float s, c;
+    sincospif(-2.0f * (float)k / (float)job.npts, &s, &c);  // k/N exact (N = 2^p)
+    out[kk] = make_float2(er + c * orr - s * oi, ei + c * oi + s * orr);
+  }
+}
+
 // Direct DFT for lengths that are not powers of two: one thread per
 // (row, bin); the phase index k n mod N is exact in 64-bit integers.
 __global__ void rdft_kernel(FftJob job) {
@@ -156,12 +331,22 @@ int rfft_bins(const FftJob& job, int nrows_out, cudaStream_t s, Scratch& sc) {
     FftJob j = job;
     j.log2n = 0;
     while ((1 << j.log2n) < job.npts) ++j.log2n;
-    const size_t smem = sizeof(float2) * (size_t)M;
-    CCFJ_CUDA_TRY(cudaFuncSetAttribute(rfft_pow2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem));
-    rfft_pow2_kernel<<<nrows_out, kFftThreads, smem, s>>>(j, tw);
-    count_launch();
-    CCFJ_LAUNCH_CHECK("rfft_pow2_kernel");
+    if (M >= kStockMinM && M <= kStockMaxM && (job.u_ld % 2) == 0 &&
+        (reinterpret_cast<uintptr_t>(job.u) % 8) == 0) {
+      const size_t smem = sizeof(float2) * (size_t)(M + M / 16);
+      CCFJ_CUDA_TRY(cudaFuncSetAttribute(rfft_stockham_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      rfft_stockham_kernel<<<nrows_out, M / 16, smem, s>>>(j, tw);
+      count_launch();
+      CCFJ_LAUNCH_CHECK("rfft_stockham_kernel");
+    } else {
+      const size_t smem = sizeof(float2) * (size_t)M;
+      CCFJ_CUDA_TRY(cudaFuncSetAttribute(rfft_pow2_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      rfft_pow2_kernel<<<nrows_out, kFftThreads, smem, s>>>(j, tw);
+      count_launch();
+      CCFJ_LAUNCH_CHECK("rfft_pow2_kernel");
+    }
   } else {
     rdft_kernel<<<dim3(nrows_out, div_up(job.nbins, 128)), 128, 0, s>>>(job);
     count_launch();

@@ -281,3 +281,43 @@ def test_wide_velocity_range(ccfj, func, zero_pair):
     y64 = _quiet(O.fj_noise, uf, r, c, f, itype=1, func=func)
     assert np.array_equal(np.isnan(y), np.isnan(y64))
     assert O.rel_error(y, y64) <= TOL
+
+
+@pytest.mark.parametrize("npts", [1024, 2048, 4096, 16384])
+def test_fj_earthquake_long_traces(ccfj, npts):
+    """Traces long enough for the 16-points-per-thread Stockham FFT (512 to
+    8192 complex points; the radix-16 passes end in a radix-2, 4, 8 or 16
+    pass): the spectra feed a transform that matches the FP64 oracle, whose
+    front end is numpy's rfft."""
+    rng = np.random.default_rng(npts)
+    Fs, ntr = 10.0, 12
+    r = np.exp(rng.uniform(np.log(2e4), np.log(4e5), ntr))
+    u = cases.ricker_records(rng, r, npts, Fs)
+    nf = 40
+    f = Fs * np.arange(nf) / npts
+    c = np.linspace(2000, 5000, 30)
+    y = _quiet(ccfj.fj_earthquake, u, r, c, f, itype=1, func=0)
+    y64 = O._normalize(O.fj_earthquake(u, r, c, f, itype=1, func=0, normalize=False))
+    assert np.array_equal(np.isnan(y), np.isnan(y64))
+    assert O.rel_error(y, y64) <= TOL
+
+
+@pytest.mark.parametrize("func", [0, 1])
+def test_mwfj_long_traces(ccfj, func):
+    """MWFJ on 16384-sample traces (the Stockham FFT of every tapered window;
+    func 0 takes the tensor-core contraction, func 1 the CUDA-core one)."""
+    rng = np.random.default_rng(91)
+    npts, Fs, ntr, nwin = 16384, 10.0, 8, 8
+    r = np.exp(rng.uniform(np.log(5e3), np.log(1.5e6), ntr))
+    L = rng.integers(200, 2001, size=(nwin, ntr))
+    start = rng.integers(0, npts - L)
+    winl, winr = start / Fs, (start + L) / Fs
+    u = cases.ricker_records(rng, r, npts, Fs)
+    f = Fs * np.arange(32) / npts
+    c = np.linspace(1500, 5000, 24)
+    y = _quiet(ccfj.MWFJ, u, r, c, f, Fs, nwin, winl, winr, taper=0.9, func=func)
+    y64 = np.stack([O._normalize(o) for o in O.MWFJ(u, r, c, f, Fs, nwin, winl, winr,
+                                                   taper=0.9, func=func, normalize=False)])
+    for w in range(nwin):
+        assert np.array_equal(np.isnan(y[w]), np.isnan(y64[w]))
+        assert O.rel_error(y[w], y64[w]) <= TOL
