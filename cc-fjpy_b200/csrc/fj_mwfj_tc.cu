@@ -380,40 +380,67 @@ __global__ void __launch_bounds__(tc::kThreads, 2) fj_mw_tc_kernel(MwTcDev a) {
   }
 }
 
-// B chunks from the windows' spectra spec[w][i][f] (complex): chunk (f, kc)
-// holds, for n = 2 w + part and K index (j, p) of interval i = 1 + 16 kc + j,
-// p = 0: g_{i-1}, p = 1: (g_i - g_{i-1}) / max(dr_i, 0.1), split into bf16
-// hi (first half of the chunk) and lo, in the K-major canonical layout.
-__global__ void mw_tc_prep_kernel(const float2* __restrict__ spec, int ntr, int nf, int nwin, int N,
-                                  int nchunks, const float* __restrict__ drs,
-                                  unsigned char* __restrict__ dst) {
-  const int fi = blockIdx.y * blockDim.x + threadIdx.x;  // frequency fastest: coalesced reads
-  const int n = blockIdx.z;                               // B row (window part)
-  const int i = 1 + blockIdx.x;                           // interval, 1 .. nchunks*16
-  if (fi >= nf) return;
-  const int w = n >> 1, part = n & 1;
-  float g0 = 0.f, b = 0.f;
-  if (w < nwin && i < ntr) {
-    const float2 cur = spec[((long long)w * ntr + i) * nf + fi];
-    const float2 prv = spec[((long long)w * ntr + i - 1) * nf + fi];
-    const float gc = part ? cur.y : cur.x, gp = part ? prv.y : prv.x;
-    g0 = gp;
-    b = (gc - gp) / fmaxf(drs[i], 0.1f);
-  }
-  const int kc = (i - 1) / tc::kChunkI, j = (i - 1) % tc::kChunkI;
+// The B operand of every (frequency, chunk of 16 intervals): window w's
+// interval data (g_{i-1}, b_i) of its real (row 2w) and imaginary (row 2w+1)
+// part, split into bf16 hi and lo, in the tensor cores' K-major tile layout.
+// One CTA builds the tiles of kPrepF consecutive frequencies and one chunk
+// in shared memory -- reading each (window, interval) for those frequencies
+// as one 32-byte piece -- then stores each frequency's tile contiguously.
+// Rows past the last window and intervals past the last pair are zero.
+constexpr int kPrepF = 4;
+__global__ void __launch_bounds__(256) mw_tc_prep_kernel(const float2* __restrict__ spec, int ntr,
+                                                         int nf, int nwin, int N, int nchunks,
+                                                         const float* __restrict__ drs,
+                                                         unsigned char* __restrict__ dst) {
+  extern __shared__ uint4 tile_u4[];
+  unsigned char* tile = reinterpret_cast<unsigned char*>(tile_u4);
+  const int kc = blockIdx.x;
+  const int f0 = blockIdx.y * kPrepF;
   const long long chunk_bytes = 2LL * tc::kSlices * N * 32;
-  unsigned char* base = dst + ((long long)fi * nchunks + kc) * chunk_bytes;
-  const int off = tile_off(n, 2 * j, N);
-  __nv_bfloat16 h0, l0, h1, l1;
-  tc::split_bf16(g0, h0, l0);
-  tc::split_bf16(b, h1, l1);
-  __nv_bfloat162 hh, ll;
-  hh.x = h0;
-  hh.y = h1;
-  ll.x = l0;
-  ll.y = l1;
-  *reinterpret_cast<__nv_bfloat162*>(base + off) = hh;
-  *reinterpret_cast<__nv_bfloat162*>(base + tc::kSlices * N * 32 + off) = ll;
+  const int half = tc::kSlices * N * 32;  // bytes of the hi (or lo) part
+  const int nw2 = N / 2;                  // window slots (rows 2w, 2w+1)
+  const int items = kPrepF * nw2 * tc::kChunkI;
+  for (int t = threadIdx.x; t < items; t += blockDim.x) {
+    const int f = t % kPrepF;
+    const int w = (t / kPrepF) % nw2;
+    const int jj = t / (kPrepF * nw2);
+    const int i = 1 + kc * tc::kChunkI + jj;  // interval i: pairs i-1, i
+    const int fi = f0 + f;
+    float g0r = 0.f, br = 0.f, g0i = 0.f, bi = 0.f;
+    if (w < nwin && i < ntr && fi < nf) {
+      const float2 cur = spec[((long long)w * ntr + i) * nf + fi];
+      const float2 prv = spec[((long long)w * ntr + i - 1) * nf + fi];
+      const float d = fmaxf(drs[i], 0.1f);  // src/FJcpu.cpp:259-261
+      g0r = prv.x;
+      br = (cur.x - prv.x) / d;
+      g0i = prv.y;
+      bi = (cur.y - prv.y) / d;
+    }
+    unsigned char* base = tile + (long long)f * chunk_bytes;
+    const float g0v[2] = {g0r, g0i}, bv[2] = {br, bi};
+#pragma unroll
+    for (int part = 0; part < 2; ++part) {
+      __nv_bfloat16 h0, l0, h1, l1;
+      tc::split_bf16(g0v[part], h0, l0);
+      tc::split_bf16(bv[part], h1, l1);
+      __nv_bfloat162 hh, ll;
+      hh.x = h0;
+      hh.y = h1;
+      ll.x = l0;
+      ll.y = l1;
+      const int off = tile_off(2 * w + part, 2 * jj, N);
+      *reinterpret_cast<__nv_bfloat162*>(base + off) = hh;
+      *reinterpret_cast<__nv_bfloat162*>(base + half + off) = ll;
+    }
+  }
+  __syncthreads();
+  const int per_f = (int)(chunk_bytes / 16);
+  for (int t = threadIdx.x; t < kPrepF * per_f; t += blockDim.x) {
+    const int f = t / per_f, q = t % per_f;
+    if (f0 + f < nf)
+      reinterpret_cast<uint4*>(dst + ((long long)(f0 + f) * nchunks + kc) * chunk_bytes)[q] =
+          tile_u4[f * per_f + q];
+  }
 }
 
 // Device flag written by the tensor-core kernel when a bounded wait ran out.
@@ -439,7 +466,10 @@ int mwfj_tensor(const ccfj_eq_args& a, const float2* spec, cudaStream_t s, Scrat
   const long long chunk_bytes = 2LL * tc::kSlices * N * 32;
   unsigned char* bch = static_cast<unsigned char*>(sc.get((size_t)nf * nchunks * chunk_bytes));
   if (!bch) return CCFJ_ERR_ALLOC;
-  mw_tc_prep_kernel<<<dim3(nchunks * tc::kChunkI, div_up(nf, 32), N), 32, 0, s>>>(
+  const size_t prep_smem = (size_t)kPrepF * chunk_bytes;
+  CCFJ_CUDA_TRY(cudaFuncSetAttribute(mw_tc_prep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)prep_smem));
+  mw_tc_prep_kernel<<<dim3(nchunks, div_up(nf, kPrepF)), 256, prep_smem, s>>>(
       spec, nr, nf, nwin, N, nchunks, drs, bch);
   count_launch();
   CCFJ_LAUNCH_CHECK("mw_tc_prep_kernel");
