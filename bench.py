@@ -513,7 +513,7 @@ def run_config(args):
                              "nf=1024, nc=2000"), seconds=t, value=terms / t)
     elif cfg == 5:
         rng = np.random.default_rng(5)
-        nsets, nf, nc = 512, 1024, 500
+        nsets, nf, nc = (64 if getattr(args, "batch_small", False) else 512), 1024, 500
         counts = np.exp(rng.uniform(np.log(50), np.log(20000), nsets)).astype(np.int64)
         off = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
         total = int(off[-1])
@@ -600,9 +600,9 @@ def run_config(args):
         res["accuracy"] = {"max_abs_err_vs_fp64_normalised": float(np.nanmax(errs)),
                            "sample": "subarrays with %s pairs" % ", ".join(str(int(counts[b]))
                                                                           for b in picks)}
-        res.update(workload="512 subarrays, %d pairs in total (log-uniform 50-20000 each), "
+        res.update(workload="%d subarrays, %d pairs in total (log-uniform 50-20000 each), "
                             "nf=1024, nc=500, itype=1 func=0; one persistent graph-replayed "
-                            "launch" % total, seconds=t_batch, value=terms / t_batch,
+                            "launch" % (nsets, total), seconds=t_batch, value=terms / t_batch,
                    separate_launches_seconds=t_sep, separate_launches_value=terms / t_sep,
                    speedup_vs_separate=t_sep / t_batch)
     print(json.dumps(res))
@@ -622,10 +622,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--profile-case", nargs="?", const="noise", default=None,
-                    choices=("noise", "mwfj"),
-                    help="run only the device transform on a reduced case (steps launches, no "
-                         "extras) for ncu captures: 'noise' = the first 512 frequencies of the "
-                         "workload; 'mwfj' = the MWFJ configuration with 8 windows and 256 bins")
+                    choices=("noise", "mwfj", "batch"),
+                    help="run a reduced case for ncu captures: 'noise' = the device transform "
+                         "on the first 512 frequencies of the workload (steps launches, no "
+                         "extras); 'mwfj' = the MWFJ configuration with 8 windows and 256 bins; "
+                         "'batch' = the ragged batch with 64 subarrays")
     ap.add_argument("--config", type=int, default=0, choices=(0, 1, 3, 4, 5),
                     help="time another workload (device-resident; one JSON line): 1 small noise array, "
                          "3 earthquake, 4 MWFJ, 5 ragged batch")
@@ -635,6 +636,10 @@ def main():
     if args.profile_case == "mwfj":
         args.config = 4
         args.mwfj_small = True
+        return run_config(args)
+    if args.profile_case == "batch":
+        args.config = 5
+        args.batch_small = True
         return run_config(args)
     if args.profile_case:
         return run_profile_case(args)
