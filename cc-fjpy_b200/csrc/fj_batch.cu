@@ -81,7 +81,7 @@ __global__ void batch_prep_u_kernel(InDesc in, const long long* __restrict__ off
         station_coef<float>(g, gl, gr, hl, hr, rs[i], hl ? rs[i - 1] : 0.0f, drs[i],
                             hr ? drs[i + 1] : 0.0f, geo[i].w, thr[fi]);
   } else {
-    static_cast<float*>(dst)[i * nf + fi] = g * wtr[i];
+    static_cast<float*>(dst)[i * nf + fi] = g * wtr[i] / geo[i].w;
   }
 }
 
@@ -153,7 +153,7 @@ __global__ void __launch_bounds__(256, fj_min_blocks<float>()) fj_batch_persiste
     a.nr = (int)(bd.off[b + 1] - o);
     a.rs += o;
     a.drs += o;
-    if (ITYPE == 1) a.geo += o;
+    a.geo += o;
     constexpr long long esz = ITYPE == 1 ? sizeof(StationCoef<float>) : sizeof(float);
     a.gb[0] = static_cast<const char*>(bd.base.gb[0]) + o * a.nf * esz;
     if (ModeTraits<MODE>::NIN > 1) a.gb[1] = static_cast<const char*>(bd.base.gb[1]) + o * a.nf * esz;
@@ -268,10 +268,10 @@ int batch_device(const ccfj_batch_args& a, long long total, cudaStream_t s) {
   const int nin = nin_of_mode(a.mode);
   float* drs = sc.get_n<float>(total + 1);
   float* wtr = sc.get_n<float>(total);
-  float4* geo = a.itype == 1 ? sc.get_n<float4>(total) : nullptr;
+  float4* geo = sc.get_n<float4>(total);
   int* order = sc.get_n<int>(a.nsets);
   unsigned long long* counter = sc.get_n<unsigned long long>(1);
-  if (!drs || !wtr || !order || !counter || (a.itype == 1 && !geo)) return CCFJ_ERR_ALLOC;
+  if (!drs || !wtr || !order || !counter || !geo) return CCFJ_ERR_ALLOC;
   CCFJ_CUDA_TRY(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s));
   if (a.nsets <= kSortMax)
     batch_order_kernel<<<1, 1024, 0, s>>>(a.offsets, a.nsets, order);

@@ -103,31 +103,36 @@ struct Cell<float> {
     fjs::eval_station_f32<WJ, WY, WZ1>(x, p_hi, p_lo, need_b, J, Y);
   }
   __device__ void prepare_folded() { s8 = (float)(8.0 / (fjs::kTwoPi * ((double)q_hi + (double)q_lo))); }
-  // gam = sqrt(2 / (pi k)): the Hankel amplitude is M = gam / sqrt(r).
-  __device__ __forceinline__ float gamma() const { return sqrtf((float)(2.0 / fjs::kPi) / k); }
+  // gam = sqrt(2 / (pi k)): the Hankel amplitude is M = gam / sqrt(r). At
+  // k = 0 (f = 0) no station reaches x >= 8 and the scale is taken as 1.
+  __device__ __forceinline__ float gamma() const {
+    return k == 0.0f ? 1.0f : sqrtf((float)(2.0 / fjs::kPi) / k);
+  }
   // Station values for the folded interval sum: y0 = Z0 / M, y1 = Z1 / M
   // with M = gam / sqrtr (rinv = 1/r and sqrtr = sqrt(r) per station;
   // sqrtr = 1 where r = 0). The range test uses s8, so x = k r is formed
-  // only below 8; LARGE asserts x >= 8 and drops the test. B is not formed.
-  template <bool WJ, bool WY, bool LARGE>
+  // only below 8; LARGE asserts x >= 8 and drops the test. B is not formed;
+  // Z1 only with WZ1.
+  template <bool WJ, bool WY, bool LARGE, bool WZ1 = true>
   __device__ __forceinline__ void eval_y(float r, float rinv, float sqrtr, ZB<float>& J,
                                          ZB<float>& Y) const {
     if (LARGE || r >= s8) {  // x >= 8
       const float p_hi = q_hi * r;
       const float e = fmaf(q_hi, r, -p_hi);
       const float p_lo = fmaf(q_lo, r, e);
-      fjs::eval_large_scaled_f32<WJ, WY, true>(s8 * rinv, p_hi, p_lo, false, 0.0f, J, Y);
+      fjs::eval_large_scaled_f32<WJ, WY, WZ1>(s8 * rinv, p_hi, p_lo, false, 0.0f, J, Y);
     } else {
-      fjs::eval_small_f32<WJ, WY, true>(k * r, false, J, Y);
-      // 1 / M = sqrtr sqrt(pi k / 2) (= sqrt(pi x / 2) for r > 0)
-      const float sc = sqrtr * fjs::sqrt_fast((float)(fjs::kPi / 2.0) * k);
+      fjs::eval_small_f32<WJ, WY, WZ1>(k * r, false, J, Y);
+      // 1 / M = sqrtr sqrt(pi k / 2) (= sqrt(pi x / 2) for r > 0; 1 / gam)
+      const float sc =
+          k == 0.0f ? sqrtr : sqrtr * fjs::sqrt_fast((float)(fjs::kPi / 2.0) * k);
       if (WJ) {
         J.z0 *= sc;
-        J.z1 *= sc;
+        if (WZ1) J.z1 *= sc;
       }
       if (WY) {
         Y.z0 *= sc;
-        Y.z1 *= sc;
+        if (WZ1) Y.z1 *= sc;
       }
     }
   }
@@ -176,14 +181,16 @@ struct Cell<double> {
     fjs::eval_station_f64<WJ, WY, WZ1>(x, q * r, J, Y);
   }
   __device__ void prepare_folded() { s8 = 8.0 / k; }
-  __device__ __forceinline__ double gamma() const { return sqrt(2.0 / (fjs::kPi * k)); }
+  __device__ __forceinline__ double gamma() const {
+    return k == 0.0 ? 1.0 : sqrt(2.0 / (fjs::kPi * k));
+  }
   // As Cell<float>::eval_y / fill_b (values divided by M = gam / sqrtr).
-  template <bool WJ, bool WY, bool LARGE>
+  template <bool WJ, bool WY, bool LARGE, bool WZ1 = true>
   __device__ __forceinline__ void eval_y(double r, double rinv, double sqrtr, ZB<double>& J,
                                          ZB<double>& Y) const {
     (void)rinv;
     fjs::eval_station_f64<WJ, WY, false>(k * r, q * r, J, Y);
-    const double sc = sqrtr * sqrt(0.5 * fjs::kPi * k);
+    const double sc = k == 0.0 ? sqrtr : sqrtr * sqrt(0.5 * fjs::kPi * k);
     if (WJ) {
       J.z0 *= sc;
       J.z1 *= sc;
@@ -347,37 +354,20 @@ __device__ __forceinline__ float4 station_geometry(float r, float d_next) {
 }
 
 // ------------------------------------------------------------ preparation
-// Gathers row perm[i] (or i) of one input, takes every u_cs-th element, and
-// writes the per-interval pair (g_{i-1}, b_i) with b_i = (g_i - g_{i-1}) /
-// max(r_i - r_{i-1}, 0.1) (src/FJcpu.cpp:259-261), or g_i * wtr_i for the
-// trapezoid.
+// itype 0: gathers row perm[i] (or i) of one input, takes every u_cs-th
+// element, and writes g_i w_i / sqrt(r_i) per (pair, frequency): the
+// trapezoid weight w (src/FJcpu.cpp:348-357) over the r part of the Hankel
+// amplitude (sqrt(r) := 1 at r = 0).
 template <typename T>
-__global__ void fj_prep_u_kernel(InDesc in, int nr, int nf, const float* __restrict__ drs,
-                                 const float* __restrict__ wtr, int itype, void* __restrict__ dst) {
+__global__ void fj_prep_u_kernel(InDesc in, int nr, int nf, const float* __restrict__ wtr,
+                                 const float4* __restrict__ geo, T* __restrict__ dst) {
   // pairs on grid x (no 65535 limit), frequencies on grid y
   const int fi = blockIdx.y * blockDim.x + threadIdx.x;
   const int i = blockIdx.x * blockDim.y + threadIdx.y;
   if (fi >= nf || i >= nr) return;
-  const long long* perm = in.perm;
-  const long long row = perm ? perm[i] : i;
+  const long long row = in.perm ? in.perm[i] : i;
   const T g = (T)in.p[row * in.ld + (long long)fi * in.cs];
-  if (itype == 1) {
-    using T2 = typename Vec2<T>::type;
-    T2 v;
-    if (i == 0) {
-      v.x = 0;
-      v.y = 0;
-    } else {
-      const long long rowp = perm ? perm[i - 1] : i - 1;
-      const T gp = (T)in.p[rowp * in.ld + (long long)fi * in.cs];
-      const T dr0 = (T)fmaxf(drs[i], 0.1f);
-      v.x = gp;
-      v.y = (g - gp) / dr0;
-    }
-    static_cast<T2*>(dst)[(long long)i * nf + fi] = v;
-  } else {
-    static_cast<T*>(dst)[(long long)i * nf + fi] = g * (T)wtr[i];
-  }
+  dst[(long long)i * nf + fi] = g * (T)wtr[i] / (T)geo[i].w;
 }
 
 // itype 1: gathers rows perm[i-1], perm[i], perm[i+1] (or i-1, i, i+1) of
@@ -556,6 +546,19 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
 }
+// Itype-0 stage: one prepared scalar per (station, frequency) per input.
+// 2 x 64 stations: 16 KB (one input) or 32 KB (two), plus the geometry.
+template <int NIN>
+struct StageBuf0 {
+  static constexpr int kStations = 64;
+  float q[2][NIN][kStations][32];
+  float4 geo[2][kStations];
+};
+
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() {
@@ -574,7 +577,7 @@ __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
   // 32 lanes stay active for the warp-wide steps below. The staged FP32
   // itype-1 loop has CTA-wide barriers: a warp past the last velocity stays
   // and helps with the staging.
-  constexpr bool kStaged = ITYPE == 1 && sizeof(T) == 4;
+  constexpr bool kStaged = sizeof(T) == 4;
   const bool c_valid = c0 < a.nc;
   if (!kStaged && !c_valid) return;
   c0 = c_valid ? c0 : 0;
@@ -589,7 +592,7 @@ __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
 #pragma unroll
   for (int j = 0; j < CPT; ++j) tot[j][0] = tot[j][1] = T(0);
   ZB<T> Jz{}, Yz{};
-  if (ITYPE == 1) {
+  if constexpr (ITYPE == 1) {
     const T thr_fold = static_cast<const T*>(a.kb)[fi];
     const StationCoef<T>* q0p = static_cast<const StationCoef<T>*>(a.gb[0]) + fi;
     const StationCoef<T>* q1p = static_cast<const StationCoef<T>*>(a.gb[MT::NIN > 1 ? 1 : 0]) + fi;
@@ -767,32 +770,107 @@ __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
       if (f_valid && c0 + j < a.nc) a.out[(long long)(c0 + j) * a.nf + fi] = v;
     }
   } else {
-    for (int i0 = 0; i0 < a.nr; i0 += kChunk) {
-      const int i1 = min(a.nr, i0 + kChunk);
-      T acc[CPT][2];
+    // Trapezoid: out = gam sum_s y0(x_s) q_s with y0 = Z0 / M and the
+    // prepared q = g w / sqrt(r) (w the trapezoid weight).
+    T s8w = T(0);
 #pragma unroll
-      for (int j = 0; j < CPT; ++j) acc[j][0] = acc[j][1] = T(0);
-      for (int i = i0; i < i1; ++i) {
-        const T r = (T)__ldg(a.rs + i);
-        const long long gidx = (long long)i * a.nf + fi;
-        const T g0 = __ldg(static_cast<const T*>(a.gb[0]) + gidx);
-        T g1 = T(0);
-        if (MT::NIN > 1) g1 = __ldg(static_cast<const T*>(a.gb[1]) + gidx);
+    for (int j = 0; j < CPT; ++j) {
+      cell[j].prepare_folded();
+      s8w = fmax(s8w, cell[j].s8);
+    }
+    for (int o = 16; o > 0; o >>= 1) s8w = fmax(s8w, __shfl_xor_sync(0xffffffffu, s8w, o));
+    const int lane = threadIdx.x & 31;
+    T acc[CPT][2];
 #pragma unroll
-        for (int j = 0; j < CPT; ++j) {
-          cell[j].template eval<WJ, WY, false>(r, cell[j].k * r, false, Jz, Yz);
-          accumulate_station<MODE, T>(acc[j], g0, g1, WJ ? Jz.z0 : T(0), WY ? Yz.z0 : T(0));
-        }
+    for (int j = 0; j < CPT; ++j) acc[j][0] = acc[j][1] = T(0);
+    auto station = [&](auto large_tag, const float4 gm, T q0, T q1) {
+      constexpr bool LARGE = decltype(large_tag)::value;
+#pragma unroll
+      for (int j = 0; j < CPT; ++j) {
+        ZB<T> Jz{}, Yz{};
+        cell[j].template eval_y<WJ, WY, LARGE, false>((T)gm.x, (T)gm.z, (T)gm.w, Jz, Yz);
+        accumulate_station<MODE, T>(acc[j], q0, q1, WJ ? Jz.z0 : T(0), WY ? Yz.z0 : T(0));
       }
+    };
+    auto flush = [&]() {
 #pragma unroll
       for (int j = 0; j < CPT; ++j) {
         tot[j][0] += acc[j][0];
         tot[j][1] += acc[j][1];
+        acc[j][0] = acc[j][1] = T(0);
+      }
+    };
+    if constexpr (kStaged) {
+      // staged as the itype-1 loop (one scalar per station and frequency)
+      using SB = StageBuf0<MT::NIN>;
+      constexpr int S = SB::kStations;
+      __shared__ SB sb;
+      const int tid = threadIdx.y * 32 + threadIdx.x;
+      const float* g0 = static_cast<const float*>(a.gb[0]);
+      const float* g1 = static_cast<const float*>(a.gb[MT::NIN > 1 ? 1 : 0]);
+      auto stage = [&](int ch, int buf) {
+        const int i0 = ch * S;
+        const int n = min(S, a.nr - i0);
+        for (int t = tid; t < n * 32; t += kCellThreads) {
+          const int st = t >> 5;
+          const long long src = (long long)(i0 + st) * a.nf + min(fbase + (t & 31), a.nf - 1);
+          cp_async4(&sb.q[buf][0][st][t & 31], g0 + src);
+          if (MT::NIN > 1) cp_async4(&sb.q[buf][MT::NIN > 1 ? 1 : 0][st][t & 31], g1 + src);
+        }
+        for (int t = tid; t < n; t += kCellThreads) cp_async16(&sb.geo[buf][t], a.geo + i0 + t);
+        cp_async_commit();
+      };
+      const int nch = (a.nr + S - 1) / S;
+      stage(0, 0);
+      for (int ch = 0; ch < nch; ++ch) {
+        const int buf = ch & 1;
+        if (ch + 1 < nch)
+          stage(ch + 1, buf ^ 1);
+        else
+          cp_async_commit();
+        cp_async_wait<1>();
+        __syncthreads();
+        const int n = min(S, a.nr - ch * S);
+        if (c_valid) {
+          float rmin = INFINITY;
+          for (int t = lane; t < n; t += 32) rmin = fminf(rmin, sb.geo[buf][t].x);
+          for (int o = 16; o > 0; o >>= 1)
+            rmin = fminf(rmin, __shfl_xor_sync(0xffffffffu, rmin, o));
+          auto run = [&](auto large_tag) {
+            CCFJ_PRAGMA(unroll CCFJ_STATION_UNROLL)
+            for (int st = 0; st < n; ++st)
+              station(large_tag, sb.geo[buf][st], sb.q[buf][0][st][lane],
+                      MT::NIN > 1 ? sb.q[buf][MT::NIN > 1 ? 1 : 0][st][lane] : 0.0f);
+          };
+          if ((T)rmin >= s8w)
+            run(BoolTag<true>{});
+          else
+            run(BoolTag<false>{});
+          flush();
+        }
+        __syncthreads();
+      }
+    } else {
+      for (int i0 = 0; i0 < a.nr; i0 += kChunk) {
+        const int i1 = min(a.nr, i0 + kChunk);
+        for (int i = i0; i < i1; ++i) {
+          const long long gidx = (long long)i * a.nf + fi;
+          const T q0 = __ldg(static_cast<const T*>(a.gb[0]) + gidx);
+          const T q1 = MT::NIN > 1 ? __ldg(static_cast<const T*>(a.gb[1]) + gidx) : T(0);
+          station(BoolTag<false>{}, __ldg(a.geo + i), q0, q1);
+        }
+        flush();
       }
     }
+    if (!c_valid) return;
 #pragma unroll
-    for (int j = 0; j < CPT; ++j)
-      if (f_valid && c0 + j < a.nc) a.out[(long long)(c0 + j) * a.nf + fi] = finish<MODE, T>(tot[j], T(1));
+    for (int j = 0; j < CPT; ++j) {
+      const T gam = cell[j].gamma();
+      T res[2];
+      res[0] = gam * tot[j][0];
+      res[1] = gam * tot[j][1];
+      if (f_valid && c0 + j < a.nc) a.out[(long long)(c0 + j) * a.nf + fi] = finish<MODE, T>(res, T(1));
+    }
   }
 }
 

@@ -266,9 +266,7 @@ void record_tuned_cpt(const ccfj_fj_args& a, int cpt) {
 
 // Bytes of the itype-1 per-station geometry and per-frequency fold
 // thresholds, and of one input's interval data.
-size_t geometry_bytes(const ccfj_fj_args& a) {
-  return a.itype == 1 ? sizeof(float4) * (size_t)a.nr : 0;
-}
+size_t geometry_bytes(const ccfj_fj_args& a) { return sizeof(float4) * (size_t)a.nr; }
 size_t kbounds_bytes(const ccfj_fj_args& a) {
   return a.itype == 1 ? (a.precision == CCFJ_PREC_FP32 ? 4 : 8) * (size_t)a.nf : 0;
 }
@@ -313,9 +311,11 @@ int prep_interval_data(const ccfj_fj_args& a, FjDev& d, const InDesc* in, int ni
       CCFJ_LAUNCH_CHECK("fj_prep_coef_kernel");
     } else {
       if (fp32)
-        fj_prep_u_kernel<float><<<pg, pb, 0, s>>>(in[j], a.nr, a.nf, d.drs, wtr, 0, g);
+        fj_prep_u_kernel<float><<<pg, pb, 0, s>>>(in[j], a.nr, a.nf, wtr, d.geo,
+                                                  static_cast<float*>(g));
       else
-        fj_prep_u_kernel<double><<<pg, pb, 0, s>>>(in[j], a.nr, a.nf, d.drs, wtr, 0, g);
+        fj_prep_u_kernel<double><<<pg, pb, 0, s>>>(in[j], a.nr, a.nf, wtr, d.geo,
+                                                   static_cast<double*>(g));
       count_launch();
       CCFJ_LAUNCH_CHECK("fj_prep_u_kernel");
     }
@@ -330,9 +330,9 @@ int fj_device(const ccfj_fj_args& a, cudaStream_t s) {
   Scratch sc(s);
   float* drs = sc.get_n<float>(a.nr + 1);
   float* wtr = sc.get_n<float>(a.nr);
-  const bool folded = a.itype == 1 && a.precision != CCFJ_PREC_FP64_PLAIN;
-  float4* geo = folded ? sc.get_n<float4>(a.nr) : nullptr;
-  if (!drs || !wtr || (folded && !geo)) return CCFJ_ERR_ALLOC;
+  const bool amortized = a.precision != CCFJ_PREC_FP64_PLAIN;
+  float4* geo = amortized ? sc.get_n<float4>(a.nr) : nullptr;
+  if (!drs || !wtr || (amortized && !geo)) return CCFJ_ERR_ALLOC;
   fj_prep_geom_kernel<<<div_up(a.nr + 1, 256), 256, 0, s>>>(a.r, a.nr, drs, wtr, geo);
   count_launch();
   CCFJ_LAUNCH_CHECK("fj_prep_geom_kernel");
@@ -957,7 +957,7 @@ static int fj_noalloc(const ccfj_fj_args& a, cudaStream_t s) {
   // kernels of this call, so nothing needs clearing between calls.
   float* drs = reinterpret_cast<float*>(p);
   float* wtr = reinterpret_cast<float*>(p + geom);
-  float4* geo = a.itype == 1 ? reinterpret_cast<float4*>(p + 2 * geom) : nullptr;
+  float4* geo = reinterpret_cast<float4*>(p + 2 * geom);
   fj_prep_geom_kernel<<<div_up(a.nr + 1, 256), 256, 0, s>>>(a.r, a.nr, drs, wtr, geo);
   count_launch();
   CCFJ_LAUNCH_CHECK("fj_prep_geom_kernel");

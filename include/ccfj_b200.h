@@ -160,10 +160,10 @@ CCFJ_API int ccfj_batch_graph_cache_clear(void);
  *
  * Its scratch is one fixed 16 MiB array in the library's device image, which
  * every GPU that loads the library holds until the process exits. It fits
- * 8 * nr (+ 16 * nr + 4 * nf for itype 1) plus, per input, 16 bytes (itype
- * 1) or 4 bytes (itype 0) per (pair, frequency): about nr * nf <= 1.04e6 for
- * one itype-1 input. Larger problems are rejected with CCFJ_ERR_INVALID and
- * a message giving both sizes.
+ * 24 * nr (+ 4 * nf for itype 1) plus, per input, 16 bytes (itype 1) or 4
+ * bytes (itype 0) per (pair, frequency): about nr * nf <= 1.04e6 for one
+ * itype-1 input. Larger problems are rejected with CCFJ_ERR_INVALID and a
+ * message giving both sizes.
  *
  * The first call on each device looks up the array's device address with
  * that device current; make that first call before any stream capture.
