@@ -24,6 +24,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <thread>
 #include <vector>
 
 #include "ccfj_core.cuh"
@@ -500,6 +501,14 @@ int host_pipe(HostPipe** out) {
   return CCFJ_OK;
 }
 
+// Host threads for gathering one block: up to 8 (half the hardware
+// threads), for blocks of at least 1024 rows.
+int gather_threads(long long rows) {
+  const unsigned hw = std::thread::hardware_concurrency();
+  const int n = (int)std::min<unsigned>(8u, hw > 1 ? hw / 2 : 1u);
+  return rows >= 1024 ? n : 1;
+}
+
 // Blocks worth splitting into: about 40 MB of spectra each (each must fit a
 // staging buffer), at least 128 frequencies each.
 int host_block_count(const ccfj_fj_args& a, long long span_floats) {
@@ -596,11 +605,25 @@ static int fj_host_blocks(const ccfj_fj_args& a, cudaStream_t s, int nblk, int n
                             cudaGetErrorString(e)));
     float* stg = static_cast<float*>(hp->stage[k]);
     const size_t row_bytes = B.width * sizeof(float);
-    for (int g = 0; g < nreg; ++g) {
-      const float* src = reg_base[g] + c_lo;
-      float* dst = stg + (size_t)g * B.width * a.u_rows;
-      for (long long row = 0; row < a.u_rows; ++row)
-        memcpy(dst + row * B.width, src + row * a.u_ld, row_bytes);
+    // the gather of the first block is on the critical path: split the rows
+    // over a few host threads
+    auto gather = [&](long long r0, long long r1) {
+      for (int g = 0; g < nreg; ++g) {
+        const float* src = reg_base[g] + c_lo;
+        float* dst = stg + (size_t)g * B.width * a.u_rows;
+        for (long long row = r0; row < r1; ++row)
+          memcpy(dst + row * B.width, src + row * a.u_ld, row_bytes);
+      }
+    };
+    const int nthr = gather_threads(a.u_rows);
+    if (nthr <= 1) {
+      gather(0, a.u_rows);
+    } else {
+      std::vector<std::thread> pool;
+      for (int t = 1; t < nthr; ++t)
+        pool.emplace_back(gather, a.u_rows * t / nthr, a.u_rows * (t + 1) / nthr);
+      gather(0, a.u_rows / nthr);
+      for (auto& th : pool) th.join();
     }
     e = cudaMemcpyAsync(B.du[0], stg, (size_t)nreg * row_bytes * a.u_rows, cudaMemcpyHostToDevice,
                         cs);
