@@ -225,16 +225,17 @@ __global__ void __launch_bounds__(kStockMaxM / 16, 2)
   TaperSpec tp;
   if (taper) tp = job.taper[row];
   // first pass (radix 16, Ns = 1): z[m] = x[2m] + i x[2m+1], m = tid + r P
+  // all 16 loads are issued before any taper arithmetic, so they overlap
   float2 v[16];
 #pragma unroll
-  for (int r = 0; r < 16; ++r) {
-    const int m = tid + r * P;
-    float2 z = __ldg(x + m);
-    if (taper) {
-      z.x *= taper_value(2 * m, tp);
-      z.y *= taper_value(2 * m + 1, tp);
+  for (int r = 0; r < 16; ++r) v[r] = __ldg(x + tid + r * P);
+  if (taper) {
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+      const int m = tid + r * P;
+      v[r].x *= taper_value(2 * m, tp);
+      v[r].y *= taper_value(2 * m + 1, tp);
     }
-    v[r] = z;
   }
   stockham_pass<16>(v, sz, M, 1, tw, tid, P);
   __syncthreads();
