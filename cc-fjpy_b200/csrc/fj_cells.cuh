@@ -591,7 +591,6 @@ __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
   T tot[CPT][2];
 #pragma unroll
   for (int j = 0; j < CPT; ++j) tot[j][0] = tot[j][1] = T(0);
-  ZB<T> Jz{}, Yz{};
   if constexpr (ITYPE == 1) {
     const T thr_fold = static_cast<const T*>(a.kb)[fi];
     const StationCoef<T>* q0p = static_cast<const StationCoef<T>*>(a.gb[0]) + fi;
