@@ -10,15 +10,18 @@
 //   trap_J / trap_Y                  src/FJcpu.cpp:323-399
 //
 // Layout in HBM (all row-major, frequency fastest, as in the reference):
-//   rs   [nr]        float  sorted distances
-//   drs  [nr]        float  r_i - r_{i-1} (drs[0] = 0)
-//   wtr  [nr]        float  trapezoid weight r_i (dr0_i + dr0_{i+1}) / 2
-//   gb   [nr][nf]    T2     (g_{i-1}, b_i) of interval (i-1, i), itype 1
-//   gw   [nr][nf]    T      g_i * wtr_i, itype 0
+//   rs   [nr]        float   sorted distances
+//   drs  [nr + 1]    float   r_i - r_{i-1} (drs[0] = drs[nr] = 0)
+//   wtr  [nr]        float   trapezoid weight r_i (dr0_i + dr0_{i+1}) / 2
+//   geo  [nr]        float4  (r_i, r_{i+1} - r_i, 1/r_i, sqrt(r_i))
+//   kb   [nf]        T       itype 1: fold threshold per frequency
+//   gb   [nr][nf]    StationCoef<T> (A, B, C, g) per station, itype 1
+//                    T       g_i wtr_i / sqrt(r_i), itype 0
 //   out  [nc][nf]    float
-// One thread owns one (f, c) cell and walks all stations in order; a warp
-// spans 32 consecutive frequencies of one velocity, so gb loads are 256-byte
-// coalesced rows and r / dr are warp-uniform broadcasts.
+// A thread owns CPT velocities of one frequency and walks all stations in
+// order; a warp spans 32 consecutive frequencies of one velocity row and a
+// CTA 8 rows, which share the chunks of station data staged in shared
+// memory (fj_cells.cuh).
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -556,7 +559,10 @@ static int fj_host_blocks(const ccfj_fj_args& a, cudaStream_t s, int nblk, int n
     float* du[2];
     float* dout;
   };
+  // Two device allocations hold every block's upload and output (one
+  // scratch entry each, whatever the number of blocks).
   Block blk[kMaxHostBlocks];
+  size_t u_total = 0;
   for (int p = 0; p < nblk; ++p) {
     Block& B = blk[p];
     // boundaries on whole warps of 32 frequencies (blocks hold >= 128)
@@ -565,14 +571,23 @@ static int fj_host_blocks(const ccfj_fj_args& a, cudaStream_t s, int nblk, int n
     const long long c_lo = (long long)(a.col_begin + B.b0) * a.fstride * a.u_es;
     const long long c_hi = (long long)(a.col_begin + B.b1 - 1) * a.fstride * a.u_es;
     B.width = c_hi - c_lo + 1 + reg_extra;
-    if ((size_t)nreg * B.width * a.u_rows * sizeof(float) > kStageBytes)
+    const size_t floats = (size_t)nreg * B.width * a.u_rows;
+    if (floats * sizeof(float) > kStageBytes)
       return set_error(CCFJ_ERR_UNSUPPORTED, "ccfj_fj_v1: host block exceeds the staging buffer");
+    u_total += (floats + 63) & ~size_t(63);  // blocks start on 256-byte boundaries
+  }
+  float* du_all = sc.get_n<float>(u_total);
+  float* dout_all = sc.get_n<float>((size_t)a.nc * a.nf);
+  if (!du_all || !dout_all) return CCFJ_ERR_ALLOC;
+  size_t u_off = 0;
+  for (int p = 0; p < nblk; ++p) {
+    Block& B = blk[p];
+    const size_t floats = (size_t)nreg * B.width * a.u_rows;
     // the block's regions are contiguous on the device (one DMA)
-    B.du[0] = sc.get_n<float>((size_t)nreg * B.width * a.u_rows);
-    if (!B.du[0]) return CCFJ_ERR_ALLOC;
+    B.du[0] = du_all + u_off;
     B.du[1] = B.du[0] + (size_t)B.width * a.u_rows;
-    B.dout = sc.get_n<float>((size_t)a.nc * (B.b1 - B.b0));
-    if (!B.dout) return CCFJ_ERR_ALLOC;
+    u_off += (floats + 63) & ~size_t(63);
+    B.dout = dout_all + (size_t)a.nc * B.b0;  // [nc][b1 - b0]
   }
   cudaEvent_t ready = nullptr, done[2] = {nullptr, nullptr};
   CCFJ_CUDA_TRY(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));

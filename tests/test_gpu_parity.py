@@ -206,19 +206,23 @@ def test_frequency_window_equals_full_transform(ccfj, func, itype):
         assert np.array_equal(part, full[:, a:b], equal_nan=True)
 
 
-@pytest.mark.parametrize("mode,merged", [(0, True), (3, True), (3, False)])
-def test_host_blocks_equal_device_path(ccfj, lib, mode, merged):
+@pytest.mark.parametrize("mode,merged,nr,nf", [(0, True, 2600, 4096), (3, True, 2600, 4096),
+                                               (3, False, 2600, 4096), (0, True, 10000, 8192)])
+def test_host_blocks_equal_device_path(ccfj, lib, mode, merged, nr, nf):
     """A host-memory transform large enough to run in frequency blocks (the
     upload of one block overlapping the transform of the previous one)
-    gives the same bits as the same transform on device-resident inputs."""
+    gives the same bits as the same transform on device-resident inputs.
+    2600 x 4096 complex spectra make 2 blocks; 10000 x 8192 make 16."""
     import torch
     from ccfj import _lib
     rng = np.random.default_rng(41)
-    nr, nf, nc = 2600, 4096, 24
+    nc = 24
     r = np.sort(rng.uniform(1e3, 3e5, nr)).astype(np.float32)
     f = np.linspace(0.01, 1.5, nf).astype(np.float32)
     c = np.linspace(800.0, 4500.0, nc).astype(np.float32)
-    uf = (rng.standard_normal((nr, nf)) + 1j * rng.standard_normal((nr, nf))).astype(np.complex64)
+    uf = np.empty((nr, nf), dtype=np.complex64)
+    uf.real = rng.standard_normal((nr, nf), dtype=np.float32)
+    uf.imag = rng.standard_normal((nr, nf), dtype=np.float32)
     perm = rng.permutation(nr).astype(np.int64)
     flat = uf.view(np.float32)                       # (nr, 2 nf): Re, Im interleaved
     if merged:
