@@ -351,8 +351,10 @@ def run_ours(args, rank, world):
 
 def run_profile_case(args):
     """The device transform on the first 512 frequencies of the workload
-    (19,900 pairs, 1000 velocities; 163 MB of spectra, 81 MB of interval
-    data: larger than L2)."""
+    (19,900 pairs, 1000 velocities; 163 MB of spectra, 163 MB of station
+    coefficients: larger than L2). With --profile-case hilbert, the func-1
+    form: J of the spectra minus Y of their Hilbert transform along the
+    512 columns."""
     import torch
     from ccfj import _lib
     lib = _lib.load()
@@ -369,6 +371,8 @@ def run_profile_case(args):
     a.struct_size = ctypes.sizeof(a)
     a.nr, a.nf, a.nc = NPAIRS, nf, NC
     a.itype, a.mode, a.precision, a.normalize, a.device_ptrs = 1, _lib.MODE_J, 0, 1, 1
+    if args.profile_case == "hilbert":
+        a.mode, a.hilbert = _lib.MODE_J_MINUS_Y, 1
     a.u[0] = d_u.data_ptr()
     a.u_ld, a.u_rows, a.u_es, a.u_ncols, a.fstride = 2 * NF, NPAIRS, 2, nf, 1
     a.perm = d_perm.data_ptr()
@@ -480,6 +484,7 @@ def run_config(args):
         a.struct_size = ctypes.sizeof(a)
         a.ntr, a.npts, a.nf, a.nc = ntr, npts, nf, nc
         a.itype, a.func, a.precision, a.normalize, a.device_ptrs, a.fstride = 1, 0, 0, 1, 1, 1
+        a.func = getattr(args, "mwfj_func", 0)  # func 1 takes the CUDA-core MWFJ kernel
         a.nwin = nwin
         a.u, a.u_ld, a.u_rows = d["u"].data_ptr(), npts, ntr
         a.perm, a.r, a.f, a.c = d["perm"].data_ptr(), d["r"].data_ptr(), d["f"].data_ptr(), \
@@ -622,20 +627,23 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--profile-case", nargs="?", const="noise", default=None,
-                    choices=("noise", "mwfj", "batch"),
+                    choices=("noise", "hilbert", "mwfj", "mwfj_cc", "batch"),
                     help="run a reduced case for ncu captures: 'noise' = the device transform "
                          "on the first 512 frequencies of the workload (steps launches, no "
                          "extras); 'mwfj' = the MWFJ configuration with 8 windows and 256 bins; "
-                         "'batch' = the ragged batch with 64 subarrays")
+                         "'hilbert' = the same with func 1 (device Hilbert transform); 'mwfj_cc' "
+                         "= the MWFJ case with func 1 (CUDA-core kernel); 'batch' = the ragged "
+                         "batch with 64 subarrays")
     ap.add_argument("--config", type=int, default=0, choices=(0, 1, 3, 4, 5),
                     help="time another workload (device-resident; one JSON line): 1 small noise array, "
                          "3 earthquake, 4 MWFJ, 5 ragged batch")
     args = ap.parse_args()
     if args.config:
         return run_config(args)
-    if args.profile_case == "mwfj":
+    if args.profile_case in ("mwfj", "mwfj_cc"):
         args.config = 4
         args.mwfj_small = True
+        args.mwfj_func = 1 if args.profile_case == "mwfj_cc" else 0
         return run_config(args)
     if args.profile_case == "batch":
         args.config = 5

@@ -19,6 +19,7 @@
 
 #include "ccfj_core.cuh"
 #include "fj_fft.cuh"
+#include "fj_frontend.cuh"
 
 namespace ccfj {
 
@@ -211,32 +212,11 @@ __device__ __forceinline__ void stockham_load(float2 (&v)[16], const float2* sz,
   }
 }
 
-__global__ void __launch_bounds__(kStockMaxM / 16, 2)
-    rfft_stockham_kernel(FftJob job, const float2* __restrict__ tw) {
-  extern __shared__ float2 sz[];
-  const int M = job.npts >> 1;
-  const int P = M >> 4;
-  const int tid = threadIdx.x;
-  const int row = blockIdx.x;
-  const int i = row % job.ntr;  // sorted trace
-  const long long src_row = job.perm ? job.perm[i] : i;
-  const float2* x = reinterpret_cast<const float2*>(job.u + src_row * job.u_ld);
-  const bool taper = job.taper != nullptr;
-  TaperSpec tp;
-  if (taper) tp = job.taper[row];
-  // first pass (radix 16, Ns = 1): z[m] = x[2m] + i x[2m+1], m = tid + r P
-  // all 16 loads are issued before any taper arithmetic, so they overlap
-  float2 v[16];
-#pragma unroll
-  for (int r = 0; r < 16; ++r) v[r] = __ldg(x + tid + r * P);
-  if (taper) {
-#pragma unroll
-    for (int r = 0; r < 16; ++r) {
-      const int m = tid + r * P;
-      v[r].x *= taper_value(2 * m, tp);
-      v[r].y *= taper_value(2 * m + 1, tp);
-    }
-  }
+// The whole M-point FFT of the 16 points per thread in v (the first pass's
+// inputs, in[tid + r P]); the result is left in natural order in sz (padded
+// indices) and the CTA is synchronised.
+__device__ __forceinline__ void stockham_fft(float2 (&v)[16], float2* sz, int M,
+                                             const float2* __restrict__ tw, int tid, int P) {
   stockham_pass<16>(v, sz, M, 1, tw, tid, P);
   __syncthreads();
   int Ns = 16;
@@ -265,6 +245,35 @@ __global__ void __launch_bounds__(kStockMaxM / 16, 2)
     }
     __syncthreads();
   }
+}
+
+__global__ void __launch_bounds__(kStockMaxM / 16, 2)
+    rfft_stockham_kernel(FftJob job, const float2* __restrict__ tw) {
+  extern __shared__ float2 sz[];
+  const int M = job.npts >> 1;
+  const int P = M >> 4;
+  const int tid = threadIdx.x;
+  const int row = blockIdx.x;
+  const int i = row % job.ntr;  // sorted trace
+  const long long src_row = job.perm ? job.perm[i] : i;
+  const float2* x = reinterpret_cast<const float2*>(job.u + src_row * job.u_ld);
+  const bool taper = job.taper != nullptr;
+  TaperSpec tp;
+  if (taper) tp = job.taper[row];
+  // first pass (radix 16, Ns = 1): z[m] = x[2m] + i x[2m+1], m = tid + r P
+  // all 16 loads are issued before any taper arithmetic, so they overlap
+  float2 v[16];
+#pragma unroll
+  for (int r = 0; r < 16; ++r) v[r] = __ldg(x + tid + r * P);
+  if (taper) {
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+      const int m = tid + r * P;
+      v[r].x *= taper_value(2 * m, tp);
+      v[r].y *= taper_value(2 * m + 1, tp);
+    }
+  }
+  stockham_fft(v, sz, M, tw, tid, P);
   // real-transform split, bins k < nbins (k <= M)
   float2* out = job.out + (long long)row * job.nbins;
   for (int kk = tid; kk < job.nbins; kk += P) {
@@ -281,6 +290,73 @@ __global__ void __launch_bounds__(kStockMaxM / 16, 2)
     sincospif(-2.0f * (float)k / (float)job.npts, &s, &c);  // k/N exact (N = 2^p)
     out[kk] = make_float2(er + c * orr - s * oi, ei + c * oi + s * orr);
   }
+}
+
+// ------------------------------------------ Hilbert transform by FFT
+// For rows of n = 512..8192 (a power of two) columns: two rows per CTA,
+// packed as z = x_a + i x_b (the transform is linear over complex scalars);
+// Z = FFT(z); bin k times +i sign(k) (scipy.fftpack.hilbert's multiplier
+// with numpy's forward sign convention; 0 at k = 0 and k = n/2); then the
+// inverse as y = conj(FFT(conj(Z'))) / n, so H(x_a) = Re y and H(x_b) = Im y.
+// O(n log n) per row instead of the direct convolution's O(n^2).
+__global__ void __launch_bounds__(kStockMaxM / 16, 2)
+    hilbert_fft_kernel(InDesc in, int n, int es, int nr, int nf, int fstride, int col_begin,
+                       const float2* __restrict__ tw, float* __restrict__ dst) {
+  extern __shared__ float2 sz[];
+  const int M = n, P = M >> 4, tid = threadIdx.x;
+  const int ia = 2 * blockIdx.x, ib = ia + 1;
+  const bool has_b = ib < nr;
+  const float* xa = in.p + (in.perm ? in.perm[ia] : ia) * in.ld;
+  const float* xb = has_b ? in.p + (in.perm ? in.perm[ib] : ib) * in.ld : xa;
+  float2 v[16];
+#pragma unroll
+  for (int r = 0; r < 16; ++r) {
+    const long long m = tid + r * P;
+    v[r] = make_float2(xa[m * es], has_b ? xb[m * es] : 0.0f);
+  }
+  stockham_fft(v, sz, M, tw, tid, P);
+  const int h = M >> 1;
+#pragma unroll
+  for (int r = 0; r < 16; ++r) {
+    const int m = tid + r * P;
+    const float2 z = sz[spad(m)];
+    // conj(Z +i) = (-z.y, -z.x) for 0 < m < n/2; conj(Z -i) = (z.y, z.x) above
+    v[r] = (m == 0 || m == h) ? make_float2(0.0f, 0.0f)
+           : m < h            ? make_float2(-z.y, -z.x)
+                              : make_float2(z.y, z.x);
+  }
+  __syncthreads();  // every read of Z is done before the second FFT writes sz
+  stockham_fft(v, sz, M, tw, tid, P);
+  const float inv_n = 1.0f / (float)n;
+  for (int j = tid; j < n; j += P) {
+    if (j % fstride) continue;
+    const int col = j / fstride - col_begin;
+    if (col < 0 || col >= nf) continue;
+    const float2 y = sz[spad(j)];
+    dst[(long long)ia * nf + col] = y.x * inv_n;
+    if (has_b) dst[(long long)ib * nf + col] = -y.y * inv_n;
+  }
+}
+
+bool hilbert_fft_supported(int n) {
+  return n >= kStockMinM && n <= kStockMaxM && (n & (n - 1)) == 0;
+}
+
+int hilbert_rows_fft(const InDesc& in, int n, int es, int nr, int nf, int fstride, int col_begin,
+                     float* dst, cudaStream_t s, Scratch& sc) {
+  float2* tw = sc.get_n<float2>(n / 2);
+  if (!tw) return CCFJ_ERR_ALLOC;
+  fft_twiddle_kernel<<<div_up(n / 2, 256), 256, 0, s>>>(n, tw);
+  count_launch();
+  CCFJ_LAUNCH_CHECK("fft_twiddle_kernel");
+  const size_t smem = sizeof(float2) * (size_t)(n + n / 16);
+  CCFJ_CUDA_TRY(cudaFuncSetAttribute(hilbert_fft_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+  hilbert_fft_kernel<<<div_up(nr, 2), n / 16, smem, s>>>(in, n, es, nr, nf, fstride, col_begin, tw,
+                                                          dst);
+  count_launch();
+  CCFJ_LAUNCH_CHECK("hilbert_fft_kernel");
+  return CCFJ_OK;
 }
 
 // Direct DFT for lengths that are not powers of two: one thread per

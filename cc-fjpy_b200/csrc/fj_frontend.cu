@@ -3,13 +3,14 @@
 //   Hilbert transform along frequency (fj_noise func=1): the reference runs
 //   scipy.fftpack.hilbert on every full row on the host
 //   (src/ccfj-gpu.pyx:258-260). For a length-n row, scipy multiplies the
-//   DFT coefficient k by -i sign(k) with the k = 0 term and, for even n, the
-//   Nyquist term set to zero. In the sample domain that is the circular
-//   convolution y[j] = sum_m h[m] x[(j - m) mod n] with
+//   DFT coefficient k (numpy's forward convention, e^{-2 pi i k m / n}) by
+//   +i sign(k), with the k = 0 term and, for even n, the Nyquist term set to
+//   zero. Rows of 512..8192 (a power of two) columns take the FFT
+//   (hilbert_rows_fft, fj_fft.cu); other lengths take the equivalent
+//   circular convolution y[j] = sum_m h[m] x[(j - m) mod n] with
 //       h[m] = -(2/n) sum_{k=1}^{K} sin(2 pi k m / n),   K = floor((n-1)/2)
 //            = -(2/n) sin(K th/2) sin((K+1) th/2) / sin(th/2),  th = 2 pi m/n
-//   (h[0] = 0). This file evaluates it directly from a shared-memory copy
-//   of the row.
+//   (h[0] = 0), evaluated directly from a shared-memory copy of the row.
 #include "ccfj_core.cuh"
 #include "fj_frontend.cuh"
 
@@ -62,13 +63,15 @@ __global__ void __launch_bounds__(kHilThreads) hilbert_rows_kernel(InDesc in, in
 #pragma unroll
     for (int t = 0; t < kHilR; ++t) acc[t] = 0.0f;
     const int jb = j0 + threadIdx.x + n;  // x2 index of output j at m = 0
+    // outputs of this pass that exist (t with j0 + 256 t < n; uniform per CTA)
+    const int tn = min(kHilR, (n - j0 + kHilThreads - 1) / kHilThreads);
     // y[j] = sum_m h[m] x2[j - m + n]; j - m + n stays in [1, 2n - 1]
     for (int m = 0; m < n; ++m) {
       const float hv = hs[m];
 #pragma unroll
       for (int t = 0; t < kHilR; ++t) {
         const int idx = jb + t * kHilThreads - m;
-        if (idx < 2 * n) acc[t] = fmaf(hv, x2[idx], acc[t]);
+        if (t < tn && idx < 2 * n) acc[t] = fmaf(hv, x2[idx], acc[t]);
       }
     }
     // keep only the columns the transform uses
@@ -83,6 +86,8 @@ __global__ void __launch_bounds__(kHilThreads) hilbert_rows_kernel(InDesc in, in
 
 int hilbert_rows(const InDesc& in, int n, int es, int nr, int nf, int fstride, int col_begin,
                  float* dst, cudaStream_t s, Scratch& sc) {
+  if (hilbert_fft_supported(n))
+    return hilbert_rows_fft(in, n, es, nr, nf, fstride, col_begin, dst, s, sc);
   if (n > kHilMaxN)
     return set_error(CCFJ_ERR_UNSUPPORTED,
                      "Hilbert transform rows longer than %d columns are not supported (got %d)",

@@ -19,6 +19,11 @@ struct InDesc {
 int hilbert_rows(const InDesc& in, int n, int es, int nr, int nf, int fstride, int col_begin,
                  float* dst, cudaStream_t s, Scratch& sc);
 
+// The same by FFT (fj_fft.cu), for n a power of two from 512 to 8192.
+bool hilbert_fft_supported(int n);
+int hilbert_rows_fft(const InDesc& in, int n, int es, int nr, int nf, int fstride, int col_begin,
+                     float* dst, cudaStream_t s, Scratch& sc);
+
 // Device-resident transform (all pointers in args are device pointers).
 int fj_device(const ccfj_fj_args& a, cudaStream_t s);
 

@@ -325,3 +325,22 @@ def test_mwfj_long_traces(ccfj, func):
     for w in range(nwin):
         assert np.array_equal(np.isnan(y[w]), np.isnan(y64[w]))
         assert O.rel_error(y[w], y64[w]) <= TOL
+
+
+@pytest.mark.parametrize("ncols,fstride", [(1024, 1), (2048, 2), (600, 1)])
+def test_func1_long_rows(ccfj, ncols, fstride):
+    """fj_noise func=1 on rows of 1024 and 2048 columns (the Hilbert
+    transform by FFT, two rows per CTA; 21 pairs leave the last row without
+    a partner) and of 600 columns (the direct convolution), against the
+    FP64 oracle built on scipy.fftpack.hilbert."""
+    rng = np.random.default_rng(ncols)
+    nr = 21
+    r = rng.uniform(2e3, 6e4, nr)
+    ff = np.linspace(0.01, 1.2, ncols)
+    uf = cases.noise_spectra(rng, r, ff, sigma=0.2)
+    f = ff[::fstride]
+    c = np.linspace(1200, 4800, 8)
+    y = _quiet(ccfj.fj_noise, uf, r, c, f, fstride=fstride, itype=1, func=1)
+    y64 = _quiet(O.fj_noise, uf, r, c, f, fstride=fstride, itype=1, func=1)
+    assert np.array_equal(np.isnan(y), np.isnan(y64))
+    assert O.rel_error(y, y64) <= TOL
