@@ -514,8 +514,8 @@ def run_config(args):
                                    "all 800 x 1024")
         res.update(workload=("fj_earthquake itype=1 func=0 with device rFFT, 500 traces x 8192 "
                              "samples, nf=1024 bins, nc=800" if cfg == 3 else
-                             "MWFJ itype=1 func=0, 1000 traces x 16384 samples, 64 windows, "
-                             "nf=1024, nc=2000"), seconds=t, value=terms / t)
+                             "MWFJ itype=1 func=%d, 1000 traces x 16384 samples, %d windows, "
+                             "nf=%d, nc=2000" % (a.func, nwin, nf)), seconds=t, value=terms / t)
     elif cfg == 5:
         rng = np.random.default_rng(5)
         nsets, nf, nc = (64 if getattr(args, "batch_small", False) else 512), 1024, 500
