@@ -514,15 +514,27 @@ int gather_threads(long long rows) {
 
 // Blocks worth splitting into: about 40 MB of spectra each (each must fit a
 // staging buffer), at least 128 frequencies each.
+// First frequency of block p (p = nblk gives nf): equal shares, with
+// boundaries on whole warps of 32 frequencies.
+static int block_start(int nf, int nblk, int p) {
+  if (p <= 0) return 0;
+  if (p >= nblk) return nf;
+  return (int)(((long long)nf * p / nblk) & ~31ll);
+}
+
 int host_block_count(const ccfj_fj_args& a, long long span_floats) {
   if (a.hilbert) return 1;
   const long long bytes = 4 * span_floats;
   int n = (int)std::min<long long>(kMaxHostBlocks, (bytes + (40ll << 20) - 1) / (40ll << 20));
   n = std::min(n, a.nf / 128);
-  // a block of nf/n frequencies spans about bytes/n (plus one column): keep
-  // that within a staging buffer
-  if (n >= 2 && bytes / n + bytes / a.nf * 2 > (long long)kStageBytes) return 1;
-  return std::max(n, 1);
+  if (n < 2) return 1;
+  // every block (its frequencies' share of the bytes, plus two columns of
+  // slack) must fit a staging buffer
+  for (int p = 0; p < n; ++p) {
+    const long long w = block_start(a.nf, n, p + 1) - block_start(a.nf, n, p);
+    if (bytes / a.nf * (w + 2) > (long long)kStageBytes) return 1;
+  }
+  return n;
 }
 }  // namespace
 
@@ -565,9 +577,8 @@ static int fj_host_blocks(const ccfj_fj_args& a, cudaStream_t s, int nblk, int n
   size_t u_total = 0;
   for (int p = 0; p < nblk; ++p) {
     Block& B = blk[p];
-    // boundaries on whole warps of 32 frequencies (blocks hold >= 128)
-    B.b0 = p == 0 ? 0 : (int)(((long long)a.nf * p / nblk) & ~31ll);
-    B.b1 = p == nblk - 1 ? a.nf : (int)(((long long)a.nf * (p + 1) / nblk) & ~31ll);
+    B.b0 = block_start(a.nf, nblk, p);
+    B.b1 = block_start(a.nf, nblk, p + 1);
     const long long c_lo = (long long)(a.col_begin + B.b0) * a.fstride * a.u_es;
     const long long c_hi = (long long)(a.col_begin + B.b1 - 1) * a.fstride * a.u_es;
     B.width = c_hi - c_lo + 1 + reg_extra;
