@@ -645,10 +645,21 @@ static int fj_host_blocks(const ccfj_fj_args& a, cudaStream_t s, int nblk, int n
     if (nthr <= 1) {
       gather(0, a.u_rows);
     } else {
+      // row ranges [start[t], start[t+1]); a thread that cannot be created
+      // leaves its range to this one (no exception crosses the C ABI)
       std::vector<std::thread> pool;
-      for (int t = 1; t < nthr; ++t)
-        pool.emplace_back(gather, a.u_rows * t / nthr, a.u_rows * (t + 1) / nthr);
+      std::vector<long long> mine;
+      for (int t = 1; t < nthr; ++t) {
+        const long long r0 = a.u_rows * t / nthr, r1 = a.u_rows * (t + 1) / nthr;
+        try {
+          pool.emplace_back(gather, r0, r1);
+        } catch (...) {
+          mine.push_back(r0);
+          mine.push_back(r1);
+        }
+      }
       gather(0, a.u_rows / nthr);
+      for (size_t q = 0; q < mine.size(); q += 2) gather(mine[q], mine[q + 1]);
       for (auto& th : pool) th.join();
     }
     e = cudaMemcpyAsync(B.du[0], stg, (size_t)nreg * row_bytes * a.u_rows, cudaMemcpyHostToDevice,
