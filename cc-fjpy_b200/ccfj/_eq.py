@@ -60,15 +60,30 @@ def _check_bins(nr, npts, nf, fstride):
 
 def _win_params(npts, Fs, T1, T2, taper):
     """Integer n1, n2, delta of the reference's `win` (src/ccfj-gpu.pyx:
-    168-178), vectorised over arrays of T1, T2 in float64 as `win` does."""
+    168-178), vectorised over arrays of T1, T2 in float64 as `win` does.
+
+    `win` zeroes out[0:n1] and out[n2:npts] (a negative n2 counts from the
+    end), then for i < delta writes sin(pi/2 i/delta) to out[n1 + i] and
+    out[n2 - 1 - i] (a negative index again counts from the end). The device
+    taper reproduces that from (n1, n2, delta); where the loop would index
+    past the array, `win` raises IndexError, and so does this."""
     n1 = np.maximum(0, np.floor(np.asarray(T1, dtype=np.float64) * Fs))
     n2 = np.minimum(npts, np.floor(np.asarray(T2, dtype=np.float64) * Fs))
     delta = np.floor((n2 - n1) * (1 - taper) / 2)
     n1i = n1.astype(np.int64)
     n2i = n2.astype(np.int64)
-    # slices out[0:n1] and out[n2:npts] clamp to [0, npts]; negative n2
-    # counts from the end in numpy, which never happens with n1 >= 0 <= n2
     di = np.maximum(delta, 0).astype(np.int64)  # range(int(delta)) is empty if < 0
+    # first loop index that leaves the array: out[n1 + i] past the end, or
+    # out[n2 - 1 - i] before -npts (the n1 write comes first within an i)
+    ia = np.maximum(npts - n1i, 0)
+    ib = np.maximum(n2i + npts, 0)
+    bad = np.minimum(ia, ib) < di
+    if np.any(bad):
+        k = np.flatnonzero(bad.ravel())[0]
+        a_, b_ = ia.ravel()[k], ib.ravel()[k]
+        idx = n1i.ravel()[k] + a_ if a_ <= b_ else n2i.ravel()[k] - 1 - b_
+        raise IndexError("index %d is out of bounds for axis 0 with size %d" % (idx, npts))
+    # beyond [-npts, npts] the slices clamp, which the device rule also does
     return (np.clip(n1i, 0, npts).astype(np.int32), np.clip(n2i, -npts, npts).astype(np.int32),
             di.astype(np.int32))
 

@@ -24,23 +24,25 @@
 namespace ccfj {
 
 // Window value at sample t for the reference's `win`, given its integer
-// n1, n2 and delta (computed on the host in float64 exactly as `win` does).
-// Where both sine ramps cover t (delta > (n2-n1)/2, taper < 0) the later
-// write of the reference's loop wins, i.e. the larger ramp index.
-__device__ __forceinline__ float taper_value(int t, const TaperSpec& w) {
-  if (t < w.n1 || t >= w.n2) return 0.0f;
-  const int i = t - w.n1;
-  const int j = w.n2 - 1 - t;
-  int m;
-  if (i < w.delta && j < w.delta)
-    m = max(i, j);
-  else if (i < w.delta)
-    m = i;
-  else if (j < w.delta)
-    m = j;
-  else
-    return 1.0f;
-  return sinpif(0.5f * (float)m / (float)w.delta);
+// n1, n2 and delta (computed on the host in float64 exactly as `win` does)
+// and the trace length npts. `win` zeroes out[0:n1] and out[n2:npts] (a
+// negative n2 counts from the end), then for i < delta writes
+// sin(pi/2 i/delta) to out[n1 + i] and out[n2 - 1 - i] (a negative index
+// again counts from the end; the host rejects loops that leave the array).
+// The value at t is that of the last write to it -- the largest iteration
+// index among t - n1, n2 - 1 - t and n2 - 1 - t + npts that lies in
+// [0, delta) -- or, without one, the zero-filled head / tail or 1.
+__device__ __forceinline__ float taper_value(int t, const TaperSpec& w, int npts) {
+  int best = -1;
+  const int ia = t - w.n1;
+  if (ia >= 0 && ia < w.delta) best = ia;
+  const int ib = w.n2 - 1 - t;
+  if (ib >= 0 && ib < w.delta) best = max(best, ib);
+  const int ibw = ib + npts;
+  if (ibw >= 0 && ibw < w.delta) best = max(best, ibw);
+  if (best >= 0) return sinpif(0.5f * (float)best / (float)w.delta);
+  const int tail = w.n2 >= 0 ? w.n2 : max(npts + w.n2, 0);
+  return (t < w.n1 || t >= tail) ? 0.0f : 1.0f;
 }
 
 // Twiddles e^{-2 pi i t / M} for t < M/2, from FP64 sinpi/cospi.
@@ -72,8 +74,8 @@ __global__ void __launch_bounds__(kFftThreads) rfft_pow2_kernel(FftJob job, cons
   for (int m = threadIdx.x; m < M; m += blockDim.x) {
     float a = x[2 * m], b = x[2 * m + 1];
     if (taper) {
-      a *= taper_value(2 * m, tp);
-      b *= taper_value(2 * m + 1, tp);
+      a *= taper_value(2 * m, tp, job.npts);
+      b *= taper_value(2 * m + 1, tp, job.npts);
     }
     z[bits > 0 ? bitrev(m, bits) : 0] = make_float2(a, b);
   }
@@ -269,8 +271,8 @@ __global__ void __launch_bounds__(kStockMaxM / 16, 2)
 #pragma unroll
     for (int r = 0; r < 16; ++r) {
       const int m = tid + r * P;
-      v[r].x *= taper_value(2 * m, tp);
-      v[r].y *= taper_value(2 * m + 1, tp);
+      v[r].x *= taper_value(2 * m, tp, job.npts);
+      v[r].y *= taper_value(2 * m + 1, tp, job.npts);
     }
   }
   stockham_fft(v, sz, M, tw, tid, P);
@@ -382,7 +384,7 @@ __global__ void rdft_kernel(FftJob job) {
   long long p = 0;  // k n mod N
   for (int n = 0; n < N; ++n) {
     float v = x[n];
-    if (taper) v *= taper_value(n, tp);
+    if (taper) v *= taper_value(n, tp, N);
     float s, c;
     sincospif(-2.0f * (float)p / (float)N, &s, &c);
     re += (double)(v * c);

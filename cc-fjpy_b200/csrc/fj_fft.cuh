@@ -5,9 +5,9 @@
 
 namespace ccfj {
 
-// One window of the reference's `win`: zero outside [n1, n2), sine ramps of
-// `delta` samples inside (all integers, computed on the host in float64 the
-// way `win` computes them).
+// One window of the reference's `win`: its n1, n2 and ramp length delta
+// (integers, computed on the host in float64 the way `win` computes them;
+// taper_value in fj_fft.cu turns them into the per-sample window).
 struct TaperSpec {
   int n1, n2, delta, pad;
 };

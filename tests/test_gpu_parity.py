@@ -344,3 +344,34 @@ def test_func1_long_rows(ccfj, ncols, fstride):
     y64 = _quiet(O.fj_noise, uf, r, c, f, fstride=fstride, itype=1, func=1)
     assert np.array_equal(np.isnan(y), np.isnan(y64))
     assert O.rel_error(y, y64) <= TOL
+
+
+@pytest.mark.parametrize("taper", [1.2, -1.5])
+def test_mwfj_degenerate_windows(ccfj, taper):
+    """Windows that end before they start (one before 0 s) with tapers
+    outside [0, 1]: the reference's win then writes ramp values outside the
+    window, and from a negative end at the end of the array. The device
+    taper reproduces them; every window matches the FP64 oracle (whose win
+    is the reference's)."""
+    from ccfj import _eq
+    rng = np.random.default_rng(61)
+    npts, Fs, ntr, nwin = 256, 10.0, 10, 3
+    r = np.exp(rng.uniform(np.log(5e3), np.log(1.5e5), ntr))
+    winl = rng.uniform(8.0, 16.0, (nwin, ntr))
+    winr = winl + rng.uniform(-6.0, 4.0, (nwin, ntr))
+    winr[0, 0] = -0.8                                 # ends before 0 s
+    for _ in range(100):                              # keep only windows win accepts
+        try:
+            _eq._win_params(npts, Fs, winl, winr, taper)
+            break
+        except IndexError:
+            winr = winl + rng.uniform(-6.0, 4.0, (nwin, ntr))
+    u = cases.ricker_records(rng, r, npts, Fs)
+    f = Fs * np.arange(24) / npts
+    c = np.linspace(1500, 5000, 20)
+    y = _quiet(ccfj.MWFJ, u, r, c, f, Fs, nwin, winl, winr, taper=taper)
+    y64 = np.stack([O._normalize(o) for o in O.MWFJ(u, r, c, f, Fs, nwin, winl, winr,
+                                                   taper=taper, normalize=False)])
+    for w in range(nwin):
+        assert np.array_equal(np.isnan(y[w]), np.isnan(y64[w]))
+        assert O.rel_error(y[w], y64[w]) <= TOL
