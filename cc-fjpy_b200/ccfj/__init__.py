@@ -15,8 +15,8 @@ host-side conventions that decide bits of the answer:
   float64 [nwin, nc, nf];
 * an unknown `func` prints the reference's message and returns 0.
 
-Not provided: `CC` (ambient-noise cross-correlation, src/CrossCorr.cpp) is
-outside this package's scope and raises NotImplementedError.
+`CC` (ambient-noise cross-correlation, src/CrossCorr.cpp) produces the
+cross-spectra that fj_noise takes (ccfj/_cc.py).
 """
 import ctypes
 import os
@@ -229,13 +229,8 @@ def GetStationPairs(nsta):
     return np.stack([ii, jj], axis=1).reshape(-1).astype(np.int32)
 
 
-def CC(*args, **kwargs):
-    """Ambient-noise cross-correlation (reference src/CrossCorr.cpp) is not
-    part of this package; compute the cross-spectra with the reference or
-    another tool and pass them to fj_noise."""
-    raise NotImplementedError("ccfj.CC (cross-correlation) is outside ccfj_b200's scope")
-
 
 from ._eq import fj_earthquake, MWFJ  # noqa: E402
 from ._batch import fj_noise_batch  # noqa: E402
+from ._cc import CC  # noqa: E402
 from . import dist  # noqa: E402,F401

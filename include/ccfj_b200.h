@@ -224,6 +224,72 @@ CCFJ_API int ccfj_device_status(void *stream);
  * device usable (CCFJ_ERR_CUDA otherwise). No counterpart in the reference. */
 CCFJ_API int ccfj_self_test_wait_timeout(void *stream);
 
+/* ---------------------------------------- ambient-noise cross-correlation
+ * The reference's CrossCorrelation (src/CrossCorr.cpp:33-159, called by CC
+ * in src/ccfj.pyx:125-147): per station, windows of fftlen samples every
+ * steplen samples (one window of npts samples when fftlen >= npts), kept
+ * where k*steplen >= startend[2i] and k*steplen + fftlen < startend[2i+1];
+ * optional one-bit (sign) of the samples; real FFT of each kept window at
+ * bins j*fstride, j < nf, optionally whitened to X/max(|X|, 1e-8); for each
+ * pair (a, b) the mean over the windows both keep of conj(X_a) X_b.
+ * Unlike the reference, bins past fftlen/2, steplen <= 0 with
+ * fftlen < npts, and pair indices outside [0, nsta) return
+ * CCFJ_ERR_INVALID. Windows of up to 16384 samples whose half length has no
+ * prime factor above 5 use a shared-memory FFT; other lengths a direct
+ * transform of the requested bins.
+ */
+typedef struct ccfj_cc_args {
+  int struct_size;     /* sizeof(ccfj_cc_args)                                 */
+  int nsta, npts;      /* stations and samples per station record              */
+  int nf, npairs;      /* output bins and station pairs                        */
+  int fstride;         /* output bin j is FFT bin j*fstride                    */
+  int fftlen, steplen; /* window length and step in samples                    */
+  int onebit;          /* nonzero: use sign(sample)                            */
+  int whiten;          /* nonzero: whiten each window's spectrum              */
+  int device_ptrs;     /* 1: data and outputs are device memory, the call is  */
+                       /*    async on `stream` (pairs and startend stay host); */
+                       /*    0: host memory, the call is synchronous and       */
+                       /*    one-bit rewrites data in place, as the reference  */
+  int accumulate;      /* 1: the sums are added to the outputs' contents       */
+                       /*    before the division (the reference's +=); pairs  */
+                       /*    with no common window keep their contents;        */
+                       /*    0: outputs are overwritten, such pairs get 0      */
+  int out_layout;      /* 0: out_re and out_im are float32 [npairs][nf];       */
+                       /* 1: out_re is complex64 [npairs][nf], out_im unused   */
+  const int *pairs;    /* host [2*npairs]: stations (a, b) of each pair        */
+  const int *startend; /* host [2*nsta]: kept sample range [start, end)        */
+  float *data;         /* [nsta][npts] float32                                 */
+  float *out_re;
+  float *out_im;
+} ccfj_cc_args;
+
+CCFJ_API int ccfj_cc_v1(const ccfj_cc_args *args, void *stream);
+
+/* Drop-in for the reference's entry (include/CrossCorr.h:13-33), with its
+ * struct layout: host memory, synchronous, ncfsr/ncfsi [npairs][nf]
+ * accumulated into and divided as the reference does, data rewritten in
+ * place by one-bit. nThreads is accepted and ignored. Returns a status
+ * (the reference always returns 0). */
+typedef struct ccfj_cc_data {
+  int nsta;
+  int npts;
+  int nf;
+  int npairs;
+  int fstride;
+  int fftlen;
+  int steplen;
+  int *Pairs;
+  int *startend;
+  float *data;
+  float *ncfsr;
+  float *ncfsi;
+  int ifonebit;
+  int ifspecwhitenning;
+  int nThreads;
+} ccfj_cc_data;
+
+CCFJ_API int CrossCorrelation(ccfj_cc_data data);
+
 /* ------------------------------------------------------------- tuning
  * The FP32 kernels come in variants that give each thread 1, 2 or 4
  * velocities. ccfj_autotune_fj_v1 runs every variant on the given problem

@@ -14,9 +14,10 @@ REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def _structs():
-    from ccfj import _batch, _eq, _lib
+    from ccfj import _batch, _cc, _eq, _lib
     return [("ccfj_fj_args", _lib.FjArgs), ("ccfj_eq_args", _eq.EqArgs),
-            ("ccfj_batch_args", _batch.BatchArgs)]
+            ("ccfj_batch_args", _batch.BatchArgs), ("ccfj_cc_args", _cc.CcArgs),
+            ("ccfj_cc_data", _cc.CcData)]
 
 
 def test_ctypes_layouts_match_header():
