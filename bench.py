@@ -386,6 +386,61 @@ def run_profile_case(args):
     return 0
 
 
+def run_cc_case(args):
+    """Cross-correlation (ccfj.CC) on the reference example's day: 200
+    stations x 345,600 samples at 4 Hz (276 MB of records), one-hour windows
+    (14,400 samples) at 0.9 overlap (steplen 1439: 231 windows per station),
+    1000 bins at fstride 3, all 19,900 pairs. Device-resident calls timed
+    with CUDA events on the launching stream, and host-memory calls
+    (ccfj.CC, copies included) timed on the wall clock. The records (276 MB)
+    and the spectra the call writes and reads (378 MB) are larger than L2."""
+    import time
+    import torch
+    import ccfj
+    from ccfj import _cc, _lib
+    lib = _lib.load()
+    nsta, fs = 200, 4
+    npts, fftlen, nf, fstride, overlap = 86400 * fs, 3600 * fs, 1000, 3, 0.9
+    data = np.random.default_rng(7).standard_normal(nsta * npts, dtype=np.float32)
+    se = np.tile([0, npts], nsta).astype(np.int32)
+    pairs = ccfj.GetStationPairs(nsta)
+    npairs = len(pairs) // 2
+    a, keep, _ = _cc._prepare(npts, nsta, nf, fftlen, pairs, se, data, overlaprate=overlap,
+                              fstride=fstride)
+    d_data = torch.from_numpy(data).cuda()
+    d_out = torch.empty((npairs, 2 * nf), dtype=torch.float32, device="cuda")
+    a.device_ptrs, a.data, a.out_re = 1, d_data.data_ptr(), d_out.data_ptr()
+    sp = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    launches0 = lib.ccfj_launch_count()
+    dev_s = _time_device(lambda: _lib.check(lib.ccfj_cc_v1(ctypes.byref(a), sp)), args.steps,
+                         args.warmup)
+    launches = (lib.ccfj_launch_count() - launches0) // (args.steps + args.warmup)
+    for _ in range(args.warmup):
+        ccfj.CC(npts, nsta, nf, fftlen, pairs, se, data, overlaprate=overlap, fstride=fstride)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ccfj.CC(npts, nsta, nf, fftlen, pairs, se, data, overlaprate=overlap, fstride=fstride)
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    nshifts = 1 + (npts - fftlen) // int(a.steplen)   # every record covers the day
+    windows = nshifts * nsta
+    fft_flops = windows * 5.0 * fftlen * np.log2(fftlen)
+    pair_flops = 8.0 * npairs * nf * nshifts
+    peak = ctypes.c_double(0)
+    _lib.check(lib.ccfj_fp32_peak_probe(sp, ctypes.byref(peak)))
+    tflops = (fft_flops + pair_flops) / dev_s / 1e12
+    print(json.dumps({
+        "case": "cc", "unit": "ms per call", "device_ms": dev_s * 1e3, "e2e_ms": e2e_s * 1e3,
+        "gpu_launches_per_call": int(launches),
+        "algorithmic_tflops": tflops, "fp32_peak_tflops": peak.value,
+        "frac_fp32": tflops / peak.value,
+        "flops": {"fft": fft_flops, "pair_products": pair_flops},
+        "config": {"workload": "CC, reference example day", "nsta": nsta, "npts": npts,
+                   "fftlen": fftlen, "steplen": int(a.steplen), "windows": windows, "nf": nf,
+                   "fstride": fstride, "npairs": npairs, "l2": "inputs larger than L2"},
+        "data": "synthetic (seeded standard normal records)"}))
+    return 0
+
+
 # ------------------------------------------------- the other configurations
 def _dev_args(lib_, torch, nr, nf, nc, itype, mode, u_ptr, u_ld, u_es, perm_ptr, r_t, f_t, c_t,
               out_t, u2_ptr=None, hilbert=0, ncols=None):
@@ -627,13 +682,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--profile-case", nargs="?", const="noise", default=None,
-                    choices=("noise", "hilbert", "mwfj", "mwfj_cc", "batch"),
+                    choices=("noise", "hilbert", "mwfj", "mwfj_cc", "batch", "cc"),
                     help="run a reduced case for ncu captures: 'noise' = the device transform "
                          "on the first 512 frequencies of the workload (steps launches, no "
                          "extras); 'mwfj' = the MWFJ configuration with 8 windows and 256 bins; "
                          "'hilbert' = the same with func 1 (device Hilbert transform); 'mwfj_cc' "
                          "= the MWFJ case with func 1 (CUDA-core kernel); 'batch' = the ragged "
-                         "batch with 64 subarrays")
+                         "batch with 64 subarrays; 'cc' = cross-correlation of the reference "
+                         "example's day (one JSON line)")
     ap.add_argument("--config", type=int, default=0, choices=(0, 1, 3, 4, 5),
                     help="time another workload (device-resident; one JSON line): 1 small noise array, "
                          "3 earthquake, 4 MWFJ, 5 ragged batch")
@@ -645,6 +701,8 @@ def main():
         args.mwfj_small = True
         args.mwfj_func = 1 if args.profile_case == "mwfj_cc" else 0
         return run_config(args)
+    if args.profile_case == "cc":
+        return run_cc_case(args)
     if args.profile_case == "batch":
         args.config = 5
         args.batch_small = True
