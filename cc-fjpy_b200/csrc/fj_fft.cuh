@@ -1,6 +1,8 @@
 // Internal interface of the time-domain front end (see fj_fft.cu).
 #pragma once
 
+#include <atomic>
+
 #include "ccfj_core.cuh"
 
 namespace ccfj {
@@ -37,6 +39,6 @@ int mwfj_tensor(const ccfj_eq_args& a, const float2* spec, cudaStream_t s, Scrat
 // Reads (and waits for) the tensor kernel's timeout flag.
 int mw_tc_error(cudaStream_t s, bool* failed);
 // 0 = automatic, 1 = CUDA cores, 2 = tensor cores where supported.
-extern int g_mwfj_path;
+extern std::atomic<int> g_mwfj_path;
 
 }  // namespace ccfj

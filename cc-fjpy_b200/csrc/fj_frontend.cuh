@@ -24,7 +24,8 @@ bool hilbert_fft_supported(int n);
 int hilbert_rows_fft(const InDesc& in, int n, int es, int nr, int nf, int fstride, int col_begin,
                      float* dst, cudaStream_t s, Scratch& sc);
 
-// Device-resident transform (all pointers in args are device pointers).
-int fj_device(const ccfj_fj_args& a, cudaStream_t s);
+// Device-resident transform (all pointers in args are device pointers);
+// cpt > 0 forces that variant of the FP32 kernel (velocities per thread).
+int fj_device(const ccfj_fj_args& a, cudaStream_t s, int cpt = 0);
 
 }  // namespace ccfj

@@ -23,6 +23,7 @@
 // CTA 8 rows, which share the chunks of station data staged in shared
 // memory (fj_cells.cuh).
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -183,8 +184,8 @@ namespace {
 // Velocities per thread of the FP32 kernel (1, 2 or 4): more share the
 // per-station loads and loop overhead, fewer keep more warps resident.
 // 0 = automatic: the tuned choice for the problem class if one is recorded
-// (ccfj_autotune_fj_v1), else 2.
-int g_force_cpt = 0;
+// (ccfj_autotune_fj_v1), else the default of default_cpt_for.
+std::atomic<int> g_force_cpt{0};
 
 template <int MODE, typename T, int CPT>
 void launch_amortized_cpt(int itype, const FjDev& d, cudaStream_t s) {
@@ -248,14 +249,14 @@ long long tune_key(const ccfj_fj_args& a) {
 }
 }  // namespace
 
-// Untuned default per mode (measured on the large-array workload): two
-// velocities per thread for one basis and one input, four for the
-// two-input Bessel form and the trapezoid, one for the two-basis forms
-// (their register use leaves too few warps resident with more).
+// Untuned default (measured on the large-array workload, with the stations
+// staged in shared memory): two velocities per thread in every itype-1 mode,
+// four for the trapezoid.
 int default_cpt_for(int mode, int itype) {
-  (void)mode;  // with the stations staged in shared memory, 2 wins in every itype-1 mode
+  (void)mode;
   return itype == 0 ? 4 : 2;
 }
+
 
 int tuned_cpt(const ccfj_fj_args& a) {
   std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -266,6 +267,14 @@ int tuned_cpt(const ccfj_fj_args& a) {
 void record_tuned_cpt(const ccfj_fj_args& a, int cpt) {
   std::lock_guard<std::mutex> lk(g_tune_mu);
   g_tune[tune_key(a)] = cpt;
+}
+
+// The variant a transform runs: the caller's choice (the autotuner's
+// candidate), else ccfj_set_fj_variant's, else the tuned or default one.
+static int variant_for(const ccfj_fj_args& a, int cpt) {
+  if (cpt > 0) return cpt;
+  const int forced = g_force_cpt.load(std::memory_order_relaxed);
+  return forced > 0 ? forced : tuned_cpt(a);
 }
 
 // Bytes of the itype-1 per-station geometry and per-frequency fold
@@ -329,7 +338,8 @@ int prep_interval_data(const ccfj_fj_args& a, FjDev& d, const InDesc* in, int ni
 }
 
 // Device-resident transform: every pointer in `a` is a device pointer.
-int fj_device(const ccfj_fj_args& a, cudaStream_t s) {
+// cpt > 0 runs that variant (velocities per thread) of the FP32 kernel.
+int fj_device(const ccfj_fj_args& a, cudaStream_t s, int cpt_choice) {
   const int nin = nin_of(a.mode);
   Scratch sc(s);
   float* drs = sc.get_n<float>(a.nr + 1);
@@ -392,7 +402,7 @@ int fj_device(const ccfj_fj_args& a, cudaStream_t s) {
     if (st != CCFJ_OK) return st;
   }
 
-  const int cpt = g_force_cpt > 0 ? g_force_cpt : tuned_cpt(a);
+  const int cpt = variant_for(a, cpt_choice);
   prof_begin(s);
   switch (a.mode) {
     case CCFJ_MODE_J:
@@ -816,7 +826,7 @@ CCFJ_API int ccfj_fj_v1(const ccfj_fj_args* args, void* stream) {
 CCFJ_API int ccfj_set_fj_variant(int cpt) {
   if (cpt != 0 && cpt != 1 && cpt != 2 && cpt != 4)
     return ccfj::set_error(CCFJ_ERR_INVALID, "ccfj_set_fj_variant: cpt must be 0, 1, 2 or 4");
-  ccfj::g_force_cpt = cpt;
+  ccfj::g_force_cpt.store(cpt, std::memory_order_relaxed);
   return CCFJ_OK;
 }
 
@@ -828,19 +838,20 @@ CCFJ_API int ccfj_autotune_fj_v1(const ccfj_fj_args* args, void* stream, int* be
   if (!args->device_ptrs)
     return ccfj::set_error(CCFJ_ERR_INVALID, "ccfj_autotune_fj_v1: needs device pointers");
   cudaStream_t s = (cudaStream_t)stream;
-  const int saved = ccfj::g_force_cpt;
   const int cands[3] = {1, 2, 4};
   int best = 2;
   float best_t = 1e30f;
-  cudaEvent_t e0, e1;
-  CCFJ_CUDA_TRY(cudaEventCreate(&e0));
-  CCFJ_CUDA_TRY(cudaEventCreate(&e1));
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    if (e0) cudaEventDestroy(e0);
+    return ccfj::set_error(CCFJ_ERR_CUDA, "ccfj_autotune_fj_v1: cudaEventCreate failed: %s",
+                           cudaGetErrorString(cudaGetLastError()));
+  }
   for (int c : cands) {
-    ccfj::g_force_cpt = c;
     float t = 1e30f;
     for (int rep = 0; rep < 3 && st == CCFJ_OK; ++rep) {
       cudaEventRecord(e0, s);
-      st = ccfj::fj_device(*args, s);
+      st = ccfj::fj_device(*args, s, c);
       cudaEventRecord(e1, s);
       if (cudaEventSynchronize(e1) != cudaSuccess) st = CCFJ_ERR_CUDA;
       float ms = 0;
@@ -853,7 +864,6 @@ CCFJ_API int ccfj_autotune_fj_v1(const ccfj_fj_args* args, void* stream, int* be
       best = c;
     }
   }
-  ccfj::g_force_cpt = saved;
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (st != CCFJ_OK) return st;
@@ -1043,7 +1053,7 @@ static int fj_noalloc(const ccfj_fj_args& a, cudaStream_t s) {
   st = prep_interval_data(a, d, in, nin, a.itype == 1 ? p + 2 * geom + gbytes : nullptr, gbuf,
                           wtr, s);
   if (st != CCFJ_OK) return st;
-  const int cpt = g_force_cpt > 0 ? g_force_cpt : tuned_cpt(a);
+  const int cpt = variant_for(a, 0);
   switch (a.mode) {
     case CCFJ_MODE_J:
       launch_mode<CCFJ_MODE_J>(a.precision, a.itype, d, nullptr, nullptr, cpt, s);
