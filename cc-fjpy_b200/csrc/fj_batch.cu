@@ -354,20 +354,69 @@ int batch_device(const ccfj_batch_args& a, long long total, cudaStream_t s) {
 }
 
 // ---------------------------------------------------------- graph cache
+// At most kMaxGraphs instantiated graphs are kept (each may hold the device
+// memory of its captured scratch allocations); capturing one more destroys
+// the least recently launched (a graph still running is freed when it ends).
+constexpr size_t kMaxGraphs = 16;
 struct GraphEntry {
   cudaGraphExec_t exec = nullptr;
+  unsigned long long last_use = 0;
 };
 std::mutex g_graph_mu;
 std::map<std::string, GraphEntry> g_graphs;
+unsigned long long g_graph_clock = 0;
 cudaStream_t g_capture_stream[64] = {};
 
+template <typename T>
+void key_put(std::string& k, const T& v) {
+  k.append(reinterpret_cast<const char*>(&v), sizeof(v));
+}
+
+// Every field of the arguments (not the struct's bytes: its padding is not
+// ours to read), the total pair count and the device.
 std::string graph_key(const ccfj_batch_args& a, long long total) {
-  std::string k(reinterpret_cast<const char*>(&a), sizeof(a));
-  k.append(reinterpret_cast<const char*>(&total), sizeof(total));
+  std::string k;
+  k.reserve(192);
+  key_put(k, a.struct_size);
+  key_put(k, a.nsets);
+  key_put(k, a.nf);
+  key_put(k, a.nc);
+  key_put(k, a.itype);
+  key_put(k, a.mode);
+  key_put(k, a.precision);
+  key_put(k, a.normalize);
+  key_put(k, a.device_ptrs);
+  key_put(k, a.hilbert);
+  key_put(k, a.use_graph);
+  key_put(k, a.variant);
+  key_put(k, a.offsets);
+  key_put(k, a.total_pairs);
+  key_put(k, a.r);
+  key_put(k, a.u[0]);
+  key_put(k, a.u[1]);
+  key_put(k, a.u_ld);
+  key_put(k, a.u_rows);
+  key_put(k, a.u_es);
+  key_put(k, a.u_ncols);
+  key_put(k, a.fstride);
+  key_put(k, a.perm);
+  key_put(k, a.f);
+  key_put(k, a.c);
+  key_put(k, a.out);
+  key_put(k, a.tau);
+  key_put(k, total);
   int dev = 0;
   cudaGetDevice(&dev);
-  k.append(reinterpret_cast<const char*>(&dev), sizeof(dev));
+  key_put(k, dev);
   return k;
+}
+
+void evict_oldest_graph() {
+  auto oldest = g_graphs.begin();
+  for (auto it = g_graphs.begin(); it != g_graphs.end(); ++it)
+    if (it->second.last_use < oldest->second.last_use) oldest = it;
+  if (oldest->second.exec) cudaGraphExecDestroy(oldest->second.exec);
+  g_graphs.erase(oldest);
 }
 
 int batch_device_graph(const ccfj_batch_args& a, long long total, cudaStream_t s) {
@@ -404,8 +453,10 @@ int batch_device_graph(const ccfj_batch_args& a, long long total, cudaStream_t s
     if (ei != cudaSuccess)
       return set_error(CCFJ_ERR_CUDA, "ccfj_fj_batch_v1: graph instantiation failed: %s",
                        cudaGetErrorString(ei));
+    if (g_graphs.size() >= kMaxGraphs) evict_oldest_graph();
     it = g_graphs.emplace(key, ge).first;
   }
+  it->second.last_use = ++g_graph_clock;
   if (s) {
     CCFJ_CUDA_TRY(cudaGraphLaunch(it->second.exec, s));
   } else {

@@ -111,9 +111,10 @@ CCFJ_API int ccfj_fj_v1(const ccfj_fj_args *args, void *stream);
  *   use_graph = 1: the launch sequence is captured once per distinct
  *     argument set into a CUDA graph and replayed on later calls (device
  *     mode; ignored when the stream is already being captured by the
- *     caller, or when a caller allocator is installed).
- *   variant: velocities per thread, 1, 2 or 4 (0 = the per-mode default of
- *     ccfj_set_fj_variant).
+ *     caller, or when a caller allocator is installed). The library keeps
+ *     the 16 most recently launched graphs and destroys older ones.
+ *   variant: velocities per thread, 1, 2 or 4 (0 = the untuned per-mode
+ *     default described at ccfj_set_fj_variant).
  * No counterpart in the reference, which has no batch entry.
  */
 typedef struct ccfj_batch_args {
