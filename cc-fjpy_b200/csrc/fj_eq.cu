@@ -52,6 +52,10 @@ static int eq_validate(const ccfj_eq_args* a) {
   CCFJ_REQUIRE(a->nwin >= 0, "ccfj_fj_earthquake_v1: nwin must be >= 0");
   CCFJ_REQUIRE(a->nwin == 0 || (a->win_n1 && a->win_n2 && a->win_delta),
                "ccfj_fj_earthquake_v1: nwin > 0 needs win_n1/win_n2/win_delta");
+  // one FFT row (and CTA) per (window, trace)
+  CCFJ_REQUIRE((long long)(a->nwin > 0 ? a->nwin : 1) * a->ntr <= 0x7fffffffLL,
+               "ccfj_fj_earthquake_v1: nwin*ntr = %lld rows exceed 2^31-1",
+               (long long)(a->nwin > 0 ? a->nwin : 1) * a->ntr);
   return CCFJ_OK;
 }
 

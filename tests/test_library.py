@@ -81,3 +81,19 @@ def test_allocator_hook_validation(lib):
         lambda n, s, u: None)
     assert lib.ccfj_set_allocator(ctypes.cast(cb, ctypes.c_void_p), None, None) == 1
     assert lib.ccfj_set_allocator(None, None, None) == 0
+
+
+def test_earthquake_rejects_more_fft_rows_than_a_grid_holds(lib):
+    """One FFT row (and CTA) per (window, trace): nwin * ntr above 2^31 - 1
+    is rejected before any device work."""
+    from ccfj import _eq
+    a = _eq.EqArgs()
+    a.struct_size = ctypes.sizeof(a)
+    a.ntr, a.npts, a.nf, a.nc = 40000, 64, 8, 4
+    a.itype, a.func, a.fstride, a.nwin = 1, 0, 1, 60000
+    a.u_ld, a.u_rows = 64, 40000
+    buf = np.zeros(64, dtype=np.float32)
+    a.u = a.r = a.f = a.c = a.out = buf.ctypes.data
+    a.win_n1 = a.win_n2 = a.win_delta = buf.ctypes.data
+    assert lib.ccfj_fj_earthquake_v1(ctypes.byref(a), None) == 1
+    assert "exceed 2^31-1" in lib.ccfj_last_error().decode()
