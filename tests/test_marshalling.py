@@ -1,0 +1,133 @@
+"""The Python layer's hand-off to ccfj_fj_v1 without a GPU: with the library
+replaced by a recorder, every element the argument struct says the device
+reads (u[0][row*u_ld + col*u_es], through the raw pointer) must equal the
+value the reference reads for that pair and frequency
+(float32(Re(uf[perm[i], j*fstride])), src/ccfj-gpu.pyx:181-200), for the
+memory layouts callers pass: complex64 read in place, float32 rows with
+any row stride, float64 / complex128 / Fortran-order copies, and the
+reference's flatten-and-reshape when the rows do not match the pairs."""
+import ctypes
+import warnings
+
+import numpy as np
+import pytest
+
+
+class _Recorder:
+    """Stands in for the loaded library: ccfj_fj_v1 reads the input through
+    the struct's pointers and strides, as the device does."""
+
+    def __init__(self):
+        self.seen = None
+
+    def ccfj_fj_v1(self, aref, stream):
+        a = aref._obj
+        nf, nr = a.nf, a.nr
+        perm = None
+        if a.perm:
+            perm = np.ctypeslib.as_array(ctypes.cast(a.perm, ctypes.POINTER(ctypes.c_longlong)),
+                                         shape=(nr,)).copy()
+        fp = ctypes.cast(a.u[0], ctypes.POINTER(ctypes.c_float))
+        vals = np.empty((nr, nf), dtype=np.float32)
+        for i in range(nr):
+            row = perm[i] if perm is not None else i
+            assert 0 <= row < a.u_rows
+            for j in range(nf):
+                col = (a.col_begin + j) * a.fstride
+                assert col < a.u_ncols
+                vals[i, j] = fp[row * a.u_ld + col * a.u_es]
+        self.seen = dict(vals=vals, es=a.u_es, ld=a.u_ld, ptr=a.u[0], fstride=a.fstride,
+                         perm=perm, mode=a.mode, hilbert=a.hilbert, normalize=a.normalize)
+        out = ctypes.cast(a.out, ctypes.POINTER(ctypes.c_float))
+        for k in range(a.nc * nf):
+            out[k] = 0.0
+        return 0
+
+    def ccfj_last_error(self):
+        return b""
+
+
+@pytest.fixture
+def rec(monkeypatch):
+    from ccfj import _lib
+    r = _Recorder()
+    monkeypatch.setattr(_lib, "load", lambda: r)
+    return r
+
+
+def _expected(uf, r, nf, fstride, sort=True):
+    idx = np.argsort(r) if sort else np.arange(len(r))
+    u = np.asarray(uf)[idx][:, ::fstride].reshape(len(r) * nf)
+    if np.iscomplexobj(u):
+        u = u.real
+    return u.astype(np.float32).reshape(len(r), nf)
+
+
+def _case(dtype, nr=7, nf=5, fstride=1, order="C", row_step=1):
+    rng = np.random.default_rng(0)
+    ncols = nf * fstride
+    base = rng.standard_normal((nr * row_step, ncols)) + 1j * rng.standard_normal(
+        (nr * row_step, ncols))
+    if not np.issubdtype(np.dtype(dtype), np.complexfloating):
+        base = base.real
+    uf = np.asarray(base, dtype=dtype, order=order)[::row_step]
+    r = rng.uniform(1e3, 5e4, nr)
+    return uf, r, np.linspace(1000, 4000, 3), np.linspace(0.1, 1.0, nf)
+
+
+@pytest.mark.parametrize("dtype,order,row_step,fstride,in_place", [
+    (np.complex64, "C", 1, 1, True),     # interleaved complex: real parts in place
+    (np.complex64, "C", 2, 3, True),     # every other row, every third column
+    (np.float32, "C", 1, 2, True),
+    (np.float32, "C", 3, 1, True),       # row stride 3 rows
+    (np.float64, "C", 1, 1, False),      # copied to float32
+    (np.complex128, "C", 1, 2, False),
+    (np.float32, "F", 1, 1, False),      # column-major: copied
+])
+def test_fj_noise_reads_what_the_reference_reads(rec, dtype, order, row_step, fstride, in_place):
+    import ccfj
+    uf, r, c, f = _case(dtype, fstride=fstride, order=order, row_step=row_step)
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        ccfj.fj_noise(uf, r, c, f, fstride=fstride)
+    s = rec.seen
+    assert np.array_equal(s["vals"], _expected(uf, r, len(f), fstride))
+    assert np.array_equal(s["perm"], np.argsort(r))
+    assert s["normalize"] == 1 and s["hilbert"] == 0
+    base = np.asarray(uf)
+    if in_place:   # no copy: the device reads the caller's memory
+        assert s["ptr"] == base.ctypes.data
+        assert s["es"] == (2 if np.iscomplexobj(base) else 1)
+    else:
+        assert s["ptr"] != base.ctypes.data
+
+
+def test_func1_asks_for_the_device_hilbert_transform(rec):
+    import ccfj
+    from ccfj import _lib
+    uf, r, c, f = _case(np.complex64)
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        ccfj.fj_noise(uf, r, c, f, func=1)
+    assert rec.seen["mode"] == _lib.MODE_J_MINUS_Y and rec.seen["hilbert"] == 1
+
+
+def test_rows_that_do_not_match_the_pairs_follow_the_reference_reshape(rec):
+    """uf with 2*nr rows of nf/2 columns holds nr*nf values: the reference's
+    uf[:, ::1].reshape(nr*nf) regroups them into nr rows of nf."""
+    import ccfj
+    rng = np.random.default_rng(1)
+    nr, nf = 6, 4
+    uf = rng.standard_normal((2 * nr, nf // 2)).astype(np.float32)
+    r = rng.uniform(1e3, 5e4, nr)
+    ccfj.fj(uf, r, np.linspace(1000, 4000, 3), np.linspace(0.1, 1.0, nf))
+    assert np.array_equal(rec.seen["vals"], uf.reshape(nr, nf))
+    assert rec.seen["perm"] is None
+
+
+def test_low_level_fj_keeps_the_callers_pair_order(rec):
+    import ccfj
+    uf, r, c, f = _case(np.float32)
+    ccfj.fhi(uf, r, c, f)
+    assert rec.seen["perm"] is None
+    assert np.array_equal(rec.seen["vals"], _expected(uf, r, len(f), 1, sort=False))
