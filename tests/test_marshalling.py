@@ -5,7 +5,10 @@ value the reference reads for that pair and frequency
 (float32(Re(uf[perm[i], j*fstride])), src/ccfj-gpu.pyx:181-200), for the
 memory layouts callers pass: complex64 read in place, float32 rows with
 any row stride, float64 / complex128 / Fortran-order copies, and the
-reference's flatten-and-reshape when the rows do not match the pairs."""
+reference's flatten-and-reshape when the rows do not match the pairs.
+Likewise for ccfj_fj_earthquake_v1: the spectra its struct describes
+(traces, permutation, MWFJ window parameters with the device's taper rule)
+equal the reference's host spectra (src/ccfj-gpu.pyx:270-313)."""
 import ctypes
 import warnings
 
@@ -131,3 +134,90 @@ def test_low_level_fj_keeps_the_callers_pair_order(rec):
     ccfj.fhi(uf, r, c, f)
     assert rec.seen["perm"] is None
     assert np.array_equal(rec.seen["vals"], _expected(uf, r, len(f), 1, sort=False))
+
+
+class _EqRecorder:
+    """Stands in for the library's ccfj_fj_earthquake_v1: reads the traces,
+    the permutation and the window parameters through the struct the way
+    the device does (sorted trace i is row perm[i]; window w of that trace
+    takes parameters [w][perm[i]] and the device's per-sample taper rule)
+    and records the spectra the transform would see."""
+
+    def __init__(self):
+        self.spec = None
+
+    def ccfj_fj_earthquake_v1(self, aref, stream):
+        from test_host_logic import _device_rule
+        a = aref._obj
+        fp = ctypes.cast(a.u, ctypes.POINTER(ctypes.c_float))
+        perm = np.ctypeslib.as_array(ctypes.cast(a.perm, ctypes.POINTER(ctypes.c_longlong)),
+                                     shape=(a.ntr,))
+        nw = max(a.nwin, 1)
+        wins = None
+        if a.nwin > 0:
+            wins = [np.ctypeslib.as_array(ctypes.cast(p, ctypes.POINTER(ctypes.c_int)),
+                                          shape=(a.nwin, a.u_rows))
+                    for p in (a.win_n1, a.win_n2, a.win_delta)]
+        spec = np.empty((nw, a.ntr, a.nf), dtype=np.complex128)
+        for w in range(nw):
+            for i in range(a.ntr):
+                row = int(perm[i])
+                x = np.array([fp[row * a.u_ld + n] for n in range(a.npts)], dtype=np.float64)
+                if wins is not None:
+                    x = x * _device_rule(a.npts, *(int(v[w, row]) for v in wins))
+                spec[w, i] = np.fft.rfft(x)[0:a.nf * a.fstride:a.fstride]
+        self.spec = spec
+        out = ctypes.cast(a.out, ctypes.POINTER(ctypes.c_float))
+        for k in range(nw * a.nc * a.nf):
+            out[k] = 0.0
+        return 0
+
+    def ccfj_last_error(self):
+        return b""
+
+
+@pytest.fixture
+def eqrec(monkeypatch):
+    from ccfj import _lib
+    r = _EqRecorder()
+    monkeypatch.setattr(_lib, "load", lambda: r)
+    return r
+
+
+def _traces(nr=6, npts=96, extra_rows=0, row_step=1, dtype=np.float32):
+    rng = np.random.default_rng(2)
+    u = rng.standard_normal(((nr + extra_rows) * row_step, npts)).astype(dtype)[::row_step]
+    return u, rng.uniform(1e3, 5e4, nr)
+
+
+@pytest.mark.parametrize("row_step,dtype", [(1, np.float32), (2, np.float32), (1, np.float64)])
+def test_fj_earthquake_spectra_are_the_references(eqrec, row_step, dtype):
+    import ccfj
+    u, r = _traces(row_step=row_step, dtype=dtype)
+    nf = 20
+    f = np.arange(nf) * 10.0 / u.shape[1]
+    ccfj.fj_earthquake(u, r, np.linspace(1000, 4000, 3), f)
+    idx = np.argsort(r)
+    ref = np.fft.rfft(u[idx].astype(np.float32).astype(np.float64))[:, 0:nf]
+    assert np.allclose(eqrec.spec[0], ref, rtol=0, atol=1e-9 * np.abs(ref).max())
+
+
+def test_mwfj_windows_follow_the_callers_trace_order(eqrec):
+    """MWFJ tapers trace j of window i by win(npts, Fs, winl[i][j],
+    winr[i][j], taper) before fj_earthquake sorts the traces
+    (src/ccfj-gpu.pyx:297-313); the device sorts first, so it must look the
+    window up by the trace's original row."""
+    import ccfj
+    u, r = _traces(nr=5, npts=120, extra_rows=2)
+    nwin, Fs, taper, nf = 3, 10.0, 0.7, 16
+    rng = np.random.default_rng(4)
+    winl = rng.uniform(-1.0, 5.0, (nwin, len(r)))
+    winr = winl + rng.uniform(2.0, 9.0, (nwin, len(r)))
+    f = np.arange(nf) * Fs / u.shape[1]
+    ccfj.MWFJ(u, r, np.linspace(1000, 4000, 3), f, Fs, nwin, winl, winr, taper=taper)
+    idx = np.argsort(r)
+    for i in range(nwin):
+        u1 = np.array([u[j] * ccfj.win(u.shape[1], Fs, winl[i][j], winr[i][j], taper)
+                       for j in range(len(r))])
+        ref = np.fft.rfft(u1[idx].astype(np.float32).astype(np.float64))[:, 0:nf]
+        assert np.allclose(eqrec.spec[i], ref, rtol=0, atol=1e-6 * np.abs(ref).max()), i
