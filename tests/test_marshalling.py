@@ -221,3 +221,54 @@ def test_mwfj_windows_follow_the_callers_trace_order(eqrec):
                        for j in range(len(r))])
         ref = np.fft.rfft(u1[idx].astype(np.float32).astype(np.float64))[:, 0:nf]
         assert np.allclose(eqrec.spec[i], ref, rtol=0, atol=1e-6 * np.abs(ref).max()), i
+
+
+class _BatchRecorder:
+    """ccfj_fj_batch_v1 stand-in: per set, the values and distances the
+    device reads for its sorted pairs."""
+
+    def __init__(self):
+        self.sets = None
+
+    def ccfj_fj_batch_v1(self, aref, stream):
+        a = aref._obj
+        P = ctypes.POINTER
+        off = np.ctypeslib.as_array(ctypes.cast(a.offsets, P(ctypes.c_longlong)),
+                                    shape=(a.nsets + 1,))
+        perm = np.ctypeslib.as_array(ctypes.cast(a.perm, P(ctypes.c_longlong)),
+                                     shape=(a.total_pairs,))
+        r = np.ctypeslib.as_array(ctypes.cast(a.r, P(ctypes.c_float)), shape=(a.total_pairs,))
+        fp = ctypes.cast(a.u[0], P(ctypes.c_float))
+        self.sets = []
+        for b in range(a.nsets):
+            vals = np.array([[fp[int(perm[i]) * a.u_ld + j * a.fstride * a.u_es]
+                              for j in range(a.nf)] for i in range(off[b], off[b + 1])],
+                            dtype=np.float32)
+            self.sets.append((vals, r[off[b]:off[b + 1]].copy()))
+        out = ctypes.cast(a.out, P(ctypes.c_float))
+        for k in range(a.nsets * a.nc * a.nf):
+            out[k] = 0.0
+        return 0
+
+    def ccfj_last_error(self):
+        return b""
+
+
+@pytest.mark.parametrize("dtype", [np.complex64, np.float64])
+def test_batch_sets_read_their_own_sorted_pairs(monkeypatch, dtype):
+    import ccfj
+    from ccfj import _lib
+    rec = _BatchRecorder()
+    monkeypatch.setattr(_lib, "load", lambda: rec)
+    rng = np.random.default_rng(5)
+    nf, fstride = 4, 2
+    ufs, rs = [], []
+    for n in (3, 1, 6):
+        x = rng.standard_normal((n, nf * fstride)) + 1j * rng.standard_normal((n, nf * fstride))
+        ufs.append(x.astype(dtype) if dtype == np.complex64 else x.real.astype(dtype))
+        rs.append(rng.uniform(1e3, 5e4, n))
+    ccfj.fj_noise_batch(ufs, rs, np.linspace(1000, 4000, 3), np.linspace(0.1, 1, nf),
+                        fstride=fstride)
+    for (vals, rsorted), uf, r in zip(rec.sets, ufs, rs):
+        assert np.array_equal(vals, _expected(uf, r, nf, fstride))
+        assert np.array_equal(rsorted, np.sort(r).astype(np.float32))
