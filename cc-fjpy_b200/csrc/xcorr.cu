@@ -245,6 +245,7 @@ static int run(const ccfj_cc_args& a, cudaStream_t s) {
   const long long nrec = (long long)a.nsta * a.npts;
   if (!a.device_ptrs && a.onebit)  // the reference rewrites the caller's samples
     for (long long n = 0; n < nrec; ++n) a.data[n] = onebit(a.data[n]);
+  if (nout == 0) return CCFJ_OK;  // no pairs or no bins: nothing for the device
 
   Scratch sc(s);
   int status = CCFJ_OK;

@@ -269,3 +269,102 @@ def test_library_rejects_pairs_outside_the_stations(lib):
     a, _keep, _out = _cc._prepare(100, 2, 5, 50, np.array([0, 2], dtype=np.int32), se, d)
     assert lib.ccfj_cc_v1(ctypes.byref(a), None) == 1
     assert "outside 0..1" in lib.ccfj_last_error().decode()
+
+
+def _smooth(m):
+    """No prime factor above 5: 2m is a length the shared-memory FFT takes."""
+    for p in (2, 3, 5):
+        while m % p == 0:
+            m //= p
+    return m == 1
+
+
+def _fuzz_case(seed):
+    rng = np.random.default_rng(1000 + seed)
+    nsta = int(rng.integers(2, 40))
+    npts = int(rng.integers(64, 1500))
+    if rng.random() < 0.6:   # the Stockham path
+        lens = [2 * m for m in range(2, (npts + 50) // 2 + 1) if _smooth(m)]
+        fftlen = int(rng.choice(lens))
+    else:                    # any length: mostly the direct transform
+        fftlen = int(rng.integers(8, npts + 50))
+    overlap = float(rng.choice([0.0, 0.25, 0.5, 0.75, 0.9]))
+    if fftlen < npts and int(fftlen * (1 - overlap)) < 1:
+        overlap = 0.0
+    F = min(fftlen, npts)
+    fstride = int(rng.integers(1, 4))
+    nf = int(rng.integers(1, (F // 2) // fstride + 2))
+    se = np.empty(2 * nsta, dtype=np.int32)   # most records cover most of the day
+    se[0::2] = rng.integers(-20, npts // 4 + 1, nsta)
+    se[1::2] = se[0::2] + rng.integers(npts // 2, npts + 40, nsta)
+    npairs = int(rng.integers(1, 3 * nsta))
+    pairs = rng.integers(0, nsta, 2 * npairs).astype(np.int32)
+    kw = dict(overlaprate=overlap, fstride=fstride, ifonebit=int(rng.integers(0, 2)),
+              ifspecwhittenning=int(rng.integers(0, 2)))
+    return (npts, nsta, nf, fftlen, pairs, se, _records(rng, nsta, npts)), kw
+
+
+def _fuzz_bounds(args, kw):
+    """Per (pair, bin): the scale of the sum's terms -- the mean over the
+    pair's common windows of |X_a| |X_b| (after one-bit and whitening), an
+    upper bound of the result that does not shrink when the terms cancel --
+    and the cells that cannot be checked: with whitening, a window whose
+    spectral value is within 1e-3 sqrt(F) of zero (one-bit samples give exact
+    zeros), which FP32 and FP64 normalise to unrelated phases."""
+    npts, nsta, nf, fftlen, pairs, se, data = args
+    steplen = int(fftlen * (1 - kw.get("overlaprate", 0.0)))
+    F, nsh = C.cc_shifts(npts, fftlen, steplen)
+    fstride, whiten = kw.get("fstride", 1), kw.get("ifspecwhittenning", 1)
+    x = data.astype(np.float64).reshape(nsta, npts)
+    if kw.get("ifonebit"):
+        x = np.sign(x)
+    mag = np.zeros((nsh, nsta, nf))
+    kept = np.zeros((nsh, nsta), dtype=bool)
+    small = np.zeros((nsta, nf), dtype=bool)
+    for i in range(nsta):
+        for k in range(nsh):
+            if C.cc_active(k, steplen, F, se, i):
+                X = np.abs(np.fft.rfft(x[i, k * steplen:k * steplen + F])[::fstride][:nf])
+                kept[k, i] = True
+                small[i] |= X < 1e-3 * np.sqrt(F)
+                mag[k, i] = np.minimum(X / np.maximum(X, 1e-8), 1.0) if whiten else X
+    # bin 0 and (even F) bin F/2 are sums of the samples with signs, exact in
+    # FP32 for one-bit samples: their zeros are zeros on both sides
+    b = np.arange(nf) * fstride
+    small &= ~((b == 0) | ((F % 2 == 0) & (b == F // 2)))[None, :]
+    pr = np.asarray(pairs)[:2 * (len(pairs) // 2)].reshape(-1, 2)
+    both = kept[:, pr[:, 0]] & kept[:, pr[:, 1]]                  # [nsh, npairs]
+    terms = (mag[:, pr[:, 0]] * mag[:, pr[:, 1]]) * both[:, :, None]
+    scale = terms.sum(axis=0) / np.maximum(both.sum(axis=0), 1)[:, None]
+    skip = (small[pr[:, 0]] | small[pr[:, 1]]) if whiten else np.zeros_like(scale, dtype=bool)
+    return scale.max(axis=1, keepdims=True), skip
+
+
+@pytest.mark.parametrize("seed", range(40))
+def test_replay_matches_oracle_fuzz(emul, seed):
+    """Random window lengths (both transforms), steps, ragged valid ranges,
+    pair lists with repeats, reversals and self-pairs, fstride, one-bit and
+    whitening: FP32 error within TOL of each pair's term scale."""
+    args, kw = _fuzz_case(seed)
+    got = _emul_cc(emul, *[np.copy(x) if isinstance(x, np.ndarray) else x for x in args], **kw)
+    ref = C.CC(*[np.copy(x) if isinstance(x, np.ndarray) else x for x in args], **kw)
+    scale, skip = _fuzz_bounds(args, kw)
+    none = scale[:, 0] == 0                    # no common window
+    assert np.all(got[none] == 0) and np.all(ref[none] == 0)
+    err = np.abs(got - ref) / np.where(scale > 0, scale, 1.0)
+    assert skip.mean() < 0.5                   # most cells are checked
+    assert err[~skip].max() <= TOL, (err[~skip].max(), kw)
+
+
+def test_calls_without_output_touch_no_device(lib):
+    """No pairs (or no bins): the library returns at once -- after one-bit
+    has rewritten the caller's samples, as the reference's loop does before
+    anything else -- so this runs without a GPU."""
+    import ccfj
+    se = np.array([0, 100, 0, 100], dtype=np.int32)
+    d = np.array(np.linspace(-1, 1, 200), dtype=np.float32)
+    out = ccfj.CC(100, 2, 5, 50, np.zeros(0, dtype=np.int32), se, d, ifonebit=1)
+    assert out.shape == (0, 5) and out.dtype == np.complex64
+    assert np.array_equal(d, np.sign(np.linspace(-1, 1, 200)).astype(np.float32))
+    out = ccfj.CC(100, 2, 0, 50, ccfj.GetStationPairs(2), se, d)
+    assert out.shape == (1, 0)
