@@ -31,7 +31,7 @@
 #define CCFJ_ERR_INVALID 1     /* bad argument (size, pointer, enum)        */
 #define CCFJ_ERR_CUDA 2        /* a CUDA runtime call or launch failed      */
 #define CCFJ_ERR_ALLOC 3       /* device or pinned allocation failed        */
-#define CCFJ_ERR_UNSUPPORTED 4 /* valid request this build cannot serve     */
+#define CCFJ_ERR_UNSUPPORTED 4 /* valid request the library cannot serve   */
 #define CCFJ_ERR_TIMEOUT 5     /* a bounded device-side wait ran out        */
 
 /* --------------------------------------------- reference-compatible entry
