@@ -28,7 +28,8 @@ from . import _lib
 from ._lib import CcfjError  # noqa: F401
 
 __all__ = ["fj_noise", "fj_earthquake", "MWFJ", "fj", "fhr", "fhi", "fh", "win",
-           "GetStationPairs", "CC", "CcfjError", "fj_noise_batch"]
+           "GetStationPairs", "CC", "CcfjError", "fj_noise_batch", "fj_full", "fHr_full",
+           "fHi_full", "fH_full", "CC_full"]
 
 _FUNC_MSG = "set func as 0 for Bessel function 1 for Hankel function"
 
@@ -233,4 +234,5 @@ def GetStationPairs(nsta):
 from ._eq import fj_earthquake, MWFJ  # noqa: E402
 from ._batch import fj_noise_batch  # noqa: E402
 from ._cc import CC  # noqa: E402
+from ._shims import CC_full, fH_full, fHi_full, fHr_full, fj_full  # noqa: E402
 from . import dist  # noqa: E402,F401

@@ -78,6 +78,11 @@ _CTYPE_NAMES = {np.dtype(np.int64): "long", np.dtype(np.int16): "short",
 def _buffer_1d(x, dtype, cname):
     """The check of a Cython typed memoryview `cname[:]`: a 1-D buffer of
     exactly that type. Returns a C-contiguous view (a copy when strided)."""
+    return np.ascontiguousarray(_buffer_1d_checked(x, dtype, cname))
+
+
+def _buffer_1d_checked(x, dtype, cname):
+    """The same check, returning the array itself (never a copy)."""
     if not isinstance(x, np.ndarray):
         try:
             memoryview(x)
@@ -89,7 +94,7 @@ def _buffer_1d(x, dtype, cname):
     if x.dtype != dtype:
         raise ValueError("Buffer dtype mismatch, expected '%s' but got '%s'"
                          % (cname, _CTYPE_NAMES.get(x.dtype, str(x.dtype))))
-    return np.ascontiguousarray(x)
+    return x
 
 
 def _prepare(npts, nsta, nf, fftlen, Pairs, startend, data, overlaprate=0.0, fstride=1,
