@@ -46,6 +46,10 @@ class BatchArgs(ctypes.Structure):
 
 _lib.SIGNATURES["ccfj_fj_batch_v1"] = (ctypes.c_int, [ctypes.POINTER(BatchArgs), ctypes.c_void_p])
 _lib.SIGNATURES["ccfj_batch_graph_cache_clear"] = (ctypes.c_int, [])
+_lib.SIGNATURES["ccfj_autotune_batch_v1"] = (ctypes.c_int, [ctypes.POINTER(BatchArgs),
+                                                             ctypes.c_void_p,
+                                                             ctypes.POINTER(ctypes.c_int),
+                                                             ctypes.POINTER(ctypes.c_float)])
 
 
 def fj_noise_batch(ufs, rs, c, f, fstride=1, itype=1, func=0, variant=0):

@@ -261,6 +261,30 @@ int batch_validate(const ccfj_batch_args* a) {
   return CCFJ_OK;
 }
 
+// Velocities per thread of the persistent kernel per batch class (mode,
+// itype and the powers of two of the total pairs, sets, nf and nc), as
+// recorded by ccfj_autotune_batch_v1; variant 0 uses it, else the untuned
+// per-mode default.
+std::mutex g_btune_mu;
+std::map<long long, int> g_btune;
+
+long long batch_tune_key(const ccfj_batch_args& a, long long total) {
+  auto lg = [](long long v) {
+    int b = 0;
+    while ((1LL << (b + 1)) <= v) ++b;
+    return (long long)b;
+  };
+  return (((((long long)a.mode * 2 + a.itype) * 64 + lg(total)) * 64 + lg(a.nsets)) * 64 +
+          lg(a.nf)) * 64 + lg(a.nc);
+}
+
+int batch_variant(const ccfj_batch_args& a, long long total) {
+  if (a.variant > 0) return a.variant;
+  std::lock_guard<std::mutex> lk(g_btune_mu);
+  auto it = g_btune.find(batch_tune_key(a, total));
+  return it == g_btune.end() ? default_cpt_for(a.mode, a.itype) : it->second;
+}
+
 // The device sequence of one batch (all pointers device pointers;
 // `total` = offsets[nsets], known to the caller).
 int batch_device(const ccfj_batch_args& a, long long total, cudaStream_t s) {
@@ -328,7 +352,7 @@ int batch_device(const ccfj_batch_args& a, long long total, cudaStream_t s) {
   bd.off = a.offsets;
   bd.order = order;
   bd.nsets = a.nsets;
-  const int cpt = a.variant > 0 ? a.variant : default_cpt_for(a.mode, a.itype);
+  const int cpt = batch_variant(a, total);
   bd.ftiles = div_up(a.nf, 32);
   bd.ctiles = div_up(a.nc, 8 * cpt);
   bd.items = (long long)a.nsets * bd.ftiles * bd.ctiles;
@@ -405,6 +429,7 @@ std::string graph_key(const ccfj_batch_args& a, long long total) {
   key_put(k, a.out);
   key_put(k, a.tau);
   key_put(k, total);
+  key_put(k, batch_variant(a, total));  // a tuning recorded later gives a new graph
   int dev = 0;
   cudaGetDevice(&dev);
   key_put(k, dev);
@@ -551,6 +576,58 @@ CCFJ_API int ccfj_fj_batch_v1(const ccfj_batch_args* args, void* stream) {
   CCFJ_REQUIRE(args->total_pairs >= args->nsets,
                "ccfj_fj_batch_v1: device mode needs total_pairs (= offsets[nsets])");
   return ccfj::batch_run_device(*args, args->total_pairs, (cudaStream_t)stream);
+}
+
+CCFJ_API int ccfj_autotune_batch_v1(const ccfj_batch_args* args, void* stream, int* best_variant,
+                                    float* best_ms) {
+  ccfj::clear_error();
+  int st = ccfj::batch_validate(args);
+  if (st != CCFJ_OK) return st;
+  CCFJ_REQUIRE(args->device_ptrs, "ccfj_autotune_batch_v1: needs device pointers");
+  CCFJ_REQUIRE(args->total_pairs >= args->nsets,
+               "ccfj_autotune_batch_v1: needs total_pairs (= offsets[nsets])");
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    if (e0) cudaEventDestroy(e0);
+    return ccfj::set_error(CCFJ_ERR_CUDA, "ccfj_autotune_batch_v1: cudaEventCreate failed: %s",
+                           cudaGetErrorString(cudaGetLastError()));
+  }
+  const int cands[3] = {1, 2, 4};
+  int best = 0;
+  float best_t = 1e30f;
+  for (int c : cands) {
+    ccfj_batch_args d = *args;
+    d.variant = c;
+    d.use_graph = 0;
+    float t = 1e30f;
+    for (int rep = 0; rep < 3 && st == CCFJ_OK; ++rep) {
+      cudaEventRecord(e0, s);
+      st = ccfj::batch_device(d, args->total_pairs, s);
+      cudaEventRecord(e1, s);
+      const cudaError_t e = cudaEventSynchronize(e1);
+      if (st == CCFJ_OK && e != cudaSuccess)
+        st = ccfj::set_error(CCFJ_ERR_CUDA, "ccfj_autotune_batch_v1: %s", cudaGetErrorString(e));
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (rep > 0) t = std::min(t, ms);  // the first run is a warm-up
+    }
+    if (st != CCFJ_OK) break;
+    if (t < best_t) {
+      best_t = t;
+      best = c;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st != CCFJ_OK) return st;
+  {
+    std::lock_guard<std::mutex> lk(ccfj::g_btune_mu);
+    ccfj::g_btune[ccfj::batch_tune_key(*args, args->total_pairs)] = best;
+  }
+  if (best_variant) *best_variant = best;
+  if (best_ms) *best_ms = best_t;
+  return CCFJ_OK;
 }
 
 CCFJ_API int ccfj_batch_graph_cache_clear(void) {

@@ -113,8 +113,9 @@ CCFJ_API int ccfj_fj_v1(const ccfj_fj_args *args, void *stream);
  *     mode; ignored when the stream is already being captured by the
  *     caller, or when a caller allocator is installed). The library keeps
  *     the 16 most recently launched graphs and destroys older ones.
- *   variant: velocities per thread, 1, 2 or 4 (0 = the untuned per-mode
- *     default described at ccfj_set_fj_variant).
+ *   variant: velocities per thread, 1, 2 or 4 (0 = the choice recorded by
+ *     ccfj_autotune_batch_v1 for the batch's class, else the untuned
+ *     per-mode default described at ccfj_set_fj_variant).
  * No counterpart in the reference, which has no batch entry.
  */
 typedef struct ccfj_batch_args {
@@ -148,6 +149,12 @@ CCFJ_API int ccfj_fj_batch_v1(const ccfj_batch_args *args, void *stream);
 /* Destroys the cached batch graphs (call before freeing buffers that a
  * cached graph refers to, if their addresses may be reused). */
 CCFJ_API int ccfj_batch_graph_cache_clear(void);
+/* Runs the batch (device pointers; out is overwritten) with 1, 2 and 4
+ * velocities per thread, records the fastest for the batch's class (mode,
+ * itype and the powers of two of total pairs, nsets, nf and nc) for later
+ * calls of this process that pass variant 0, and returns it and its time. */
+CCFJ_API int ccfj_autotune_batch_v1(const ccfj_batch_args *args, void *stream,
+                                    int *best_variant, float *best_ms);
 
 /* ------------------------------------------ allocation-free transform
  * No counterpart in the reference. The same FP32 transform as ccfj_fj_v1

@@ -97,3 +97,26 @@ def test_earthquake_rejects_more_fft_rows_than_a_grid_holds(lib):
     a.win_n1 = a.win_n2 = a.win_delta = buf.ctypes.data
     assert lib.ccfj_fj_earthquake_v1(ctypes.byref(a), None) == 1
     assert "exceed 2^31-1" in lib.ccfj_last_error().decode()
+
+
+def test_batch_autotuner_needs_device_pointers(lib):
+    """ccfj_autotune_batch_v1 validates like the batch entry and times only
+    device-resident batches (host-memory calls would time the copies)."""
+    from ccfj import _batch
+    a = _batch.BatchArgs()
+    a.struct_size = ctypes.sizeof(a)
+    a.nsets, a.nf, a.nc, a.itype, a.mode = 1, 4, 2, 1, 0
+    buf = np.zeros(64, dtype=np.float32)
+    offsets = np.array([0, 3], dtype=np.int64)
+    a.offsets = offsets.ctypes.data
+    a.r = a.f = a.c = a.out = buf.ctypes.data
+    a.u[0] = buf.ctypes.data
+    a.u_ld, a.u_rows, a.u_es, a.u_ncols, a.fstride = 4, 3, 1, 4, 1
+    best, ms = ctypes.c_int(), ctypes.c_float()
+    assert lib.ccfj_autotune_batch_v1(ctypes.byref(a), None, ctypes.byref(best),
+                                      ctypes.byref(ms)) == 1
+    assert "device pointers" in lib.ccfj_last_error().decode()
+    a.variant = 3
+    assert lib.ccfj_autotune_batch_v1(ctypes.byref(a), None, ctypes.byref(best),
+                                      ctypes.byref(ms)) == 1
+    assert "variant" in lib.ccfj_last_error().decode()
