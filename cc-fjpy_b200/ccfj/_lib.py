@@ -77,6 +77,10 @@ SIGNATURES = {
     "ccfj_last_transform_ms": (ctypes.c_float, []),
     "ccfj_profile_total_ms": (ctypes.c_double, [ctypes.POINTER(ctypes.c_int)]),
     "ccfj_fp32_peak_probe": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]),
+}
+
+# the unit tests' probe library (include/ccfj_b200_probe.h)
+PROBE_SIGNATURES = {
     "ccfj_special_host": (ctypes.c_int, [ctypes.c_int, ctypes.c_longlong,
                                          ctypes.POINTER(ctypes.c_double),
                                          ctypes.POINTER(ctypes.c_double)]),
@@ -91,23 +95,41 @@ def lib_path():
     return _build.LIB
 
 
+def _bind(lib, signatures):
+    for name, (res, args) in signatures.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
 def load():
-    """Returns the loaded library (building it first if it is absent)."""
+    """Returns the loaded library, building it first if it is absent or was
+    built from other sources than the ones in this tree."""
     global _LIB
     if _LIB is not None:
         return _LIB
     path = os.environ.get("CCFJ_LIB_PATH") or _build.LIB
-    if not os.path.exists(path):
-        if path != _build.LIB:
-            raise FileNotFoundError("CCFJ_LIB_PATH=%s does not exist" % path)
-        _build.build()
-    lib = ctypes.CDLL(path)
-    for name, (res, args) in SIGNATURES.items():
-        fn = getattr(lib, name)
-        fn.restype = res
-        fn.argtypes = args
-    _LIB = lib
-    return lib
+    if path == _build.LIB:
+        if not _build.up_to_date():
+            _build.build()
+    elif not os.path.exists(path):
+        raise FileNotFoundError("CCFJ_LIB_PATH=%s does not exist" % path)
+    _LIB = _bind(ctypes.CDLL(path), SIGNATURES)
+    return _LIB
+
+
+_PROBE = None
+
+
+def load_probe():
+    """The unit tests' special-function probe library (not the product)."""
+    global _PROBE
+    if _PROBE is None:
+        if not _build.up_to_date(_build.PROBE_LIB, _build.probe_sources()):
+            _build.build()
+        _PROBE = _bind(ctypes.CDLL(_build.PROBE_LIB), PROBE_SIGNATURES)
+    return _PROBE
 
 
 class CcfjError(RuntimeError):

@@ -390,6 +390,9 @@ std::mutex g_graph_mu;
 std::map<std::string, GraphEntry> g_graphs;
 unsigned long long g_graph_clock = 0;
 cudaStream_t g_capture_stream[64] = {};
+// per device: stream 0 -> library stream, library stream -> stream 0
+// (used under g_graph_mu)
+cudaEvent_t g_order_event[64][2] = {};
 
 template <typename T>
 void key_put(std::string& k, const T& v) {
@@ -485,11 +488,23 @@ int batch_device_graph(const ccfj_batch_args& a, long long total, cudaStream_t s
   if (s) {
     CCFJ_CUDA_TRY(cudaGraphLaunch(it->second.exec, s));
   } else {
+    // The legacy default stream cannot launch a captured graph's work in
+    // order by itself, and the library stream is non-blocking: order the
+    // launch after the caller's earlier default-stream work, and the
+    // caller's later default-stream work after the launch, with events (no
+    // host synchronisation), as a kernel launched on stream 0 would be.
     int dev = 0;
     CCFJ_CUDA_TRY(cudaGetDevice(&dev));
     cudaStream_t cap = g_capture_stream[dev];
+    if (!g_order_event[dev][0]) {
+      CCFJ_CUDA_TRY(cudaEventCreateWithFlags(&g_order_event[dev][0], cudaEventDisableTiming));
+      CCFJ_CUDA_TRY(cudaEventCreateWithFlags(&g_order_event[dev][1], cudaEventDisableTiming));
+    }
+    CCFJ_CUDA_TRY(cudaEventRecord(g_order_event[dev][0], 0));
+    CCFJ_CUDA_TRY(cudaStreamWaitEvent(cap, g_order_event[dev][0], 0));
     CCFJ_CUDA_TRY(cudaGraphLaunch(it->second.exec, cap));
-    CCFJ_CUDA_TRY(cudaStreamSynchronize(cap));
+    CCFJ_CUDA_TRY(cudaEventRecord(g_order_event[dev][1], cap));
+    CCFJ_CUDA_TRY(cudaStreamWaitEvent(0, g_order_event[dev][1], 0));
   }
   count_launch();
   return CCFJ_OK;

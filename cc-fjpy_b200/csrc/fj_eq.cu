@@ -59,8 +59,9 @@ static int eq_validate(const ccfj_eq_args* a) {
   return CCFJ_OK;
 }
 
-// All pointers device pointers.
-static int eq_device(const ccfj_eq_args& a, cudaStream_t s) {
+// All pointers device pointers. call_err: a device word that receives this
+// call's timeout flag of the tensor-core path (NULL: scratch of the call).
+static int eq_device(const ccfj_eq_args& a, cudaStream_t s, unsigned int* call_err = nullptr) {
   Scratch sc(s);
   const int nw = a.nwin > 0 ? a.nwin : 1;
   const long long rows_out = (long long)nw * a.ntr;
@@ -95,7 +96,7 @@ static int eq_device(const ccfj_eq_args& a, cudaStream_t s) {
     const bool tc_ok = a.itype == 1 && a.func == 0 && a.ntr >= 2 && a.nwin <= 128;
     const int path = g_mwfj_path.load(std::memory_order_relaxed);
     const bool use_tc = tc_ok && (path == 2 || (path == 0 && a.nwin >= 8));
-    if (use_tc) return mwfj_tensor(a, spec, s, sc);
+    if (use_tc) return mwfj_tensor(a, spec, s, sc, call_err);
     return mwfj_cuda_core(a, spec, s, sc);
   }
 
@@ -146,7 +147,9 @@ static int eq_host(const ccfj_eq_args& a, cudaStream_t s) {
   float* df = sc.get_n<float>(a.nf);
   float* dc = sc.get_n<float>(a.nc);
   float* dout = sc.get_n<float>((size_t)nw * a.nc * a.nf);
-  if (!du || !dr || !df || !dc || !dout) return CCFJ_ERR_ALLOC;
+  unsigned int* derr = sc.get_n<unsigned int>(1);
+  if (!du || !dr || !df || !dc || !dout || !derr) return CCFJ_ERR_ALLOC;
+  CCFJ_CUDA_TRY(cudaMemsetAsync(derr, 0, sizeof(unsigned int), s));
   CCFJ_CUDA_TRY(cudaMemcpyAsync(du, a.u, ubytes, cudaMemcpyHostToDevice, s));
   CCFJ_CUDA_TRY(cudaMemcpyAsync(dr, a.r, sizeof(float) * a.ntr, cudaMemcpyHostToDevice, s));
   CCFJ_CUDA_TRY(cudaMemcpyAsync(df, a.f, sizeof(float) * a.nf, cudaMemcpyHostToDevice, s));
@@ -175,13 +178,12 @@ static int eq_host(const ccfj_eq_args& a, cudaStream_t s) {
   d.f = df;
   d.c = dc;
   d.out = dout;
-  int st = eq_device(d, s);
+  int st = eq_device(d, s, derr);
   if (st != CCFJ_OK) return st;
   CCFJ_CUDA_TRY(cudaMemcpyAsync(a.out, dout, sizeof(float) * nw * a.nc * a.nf,
                                 cudaMemcpyDeviceToHost, s));
-  CCFJ_CUDA_TRY(cudaStreamSynchronize(s));
   bool failed = false;
-  st = mw_tc_error(s, &failed);
+  st = mw_tc_call_error(derr, s, &failed);
   if (st != CCFJ_OK) return st;
   if (failed)
     return set_error(CCFJ_ERR_TIMEOUT, "ccfj_fj_earthquake_v1: a bounded device wait ran out");
@@ -202,7 +204,7 @@ CCFJ_API int ccfj_set_mwfj_path(int path) {
 CCFJ_API int ccfj_device_status(void* stream) {
   ccfj::clear_error();
   bool failed = false;
-  const int st = ccfj::mw_tc_error((cudaStream_t)stream, &failed);
+  const int st = ccfj::mw_tc_sticky_error((cudaStream_t)stream, &failed);
   if (st != CCFJ_OK) return st;
   if (failed) return ccfj::set_error(CCFJ_ERR_TIMEOUT, "a bounded device wait ran out");
   return CCFJ_OK;

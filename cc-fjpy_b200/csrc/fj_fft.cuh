@@ -35,9 +35,14 @@ int rfft_bins(const FftJob& job, int nrows_out, cudaStream_t s, Scratch& sc);
 int mwfj_cuda_core(const ccfj_eq_args& a, const float2* spec, cudaStream_t s, Scratch& sc);
 // The same contraction on the tensor cores (tcgen05, BF16x3): itype 1,
 // func 0, 2 <= nr, nwin <= 128.
-int mwfj_tensor(const ccfj_eq_args& a, const float2* spec, cudaStream_t s, Scratch& sc);
-// Reads (and waits for) the tensor kernel's timeout flag.
-int mw_tc_error(cudaStream_t s, bool* failed);
+// call_err: a device word for this call's timeout flag (NULL: taken from sc).
+int mwfj_tensor(const ccfj_eq_args& a, const float2* spec, cudaStream_t s, Scratch& sc,
+                unsigned int* call_err);
+// Waits for `s` and reads one call's timeout flag.
+int mw_tc_call_error(const unsigned int* err, cudaStream_t s, bool* failed);
+// Waits for `s`, reads the process-wide timeout flag of the tensor kernel
+// (set by any call since the last read) and clears it.
+int mw_tc_sticky_error(cudaStream_t s, bool* failed);
 // 0 = automatic, 1 = CUDA cores, 2 = tensor cores where supported.
 extern std::atomic<int> g_mwfj_path;
 

@@ -162,7 +162,8 @@ struct MwTcDev {
   const float* f;
   const float* c;
   float* out;               // [nwin][nc][nf]
-  unsigned int* err;        // set to 1 when a bounded wait runs out
+  unsigned int* err;        // this call's flag: set to 1 when a bounded wait runs out
+  unsigned int* sticky;     // process-wide flag (g_mw_tc_error) set alongside, or NULL
   int nr, nf, nc, nwin;
   int N;                    // 2 nwin padded to a multiple of 16
   int nchunks;              // ceil((nr - 1) / kChunkI)
@@ -371,6 +372,7 @@ __global__ void __launch_bounds__(tc::kThreads, 2) fj_mw_tc_kernel(MwTcDev a) {
     }
   } else if (tid == 0) {
     atomicOr(a.err, 1u);
+    if (a.sticky) atomicOr(a.sticky, 1u);
   }
   tc::tc_fence_before();
   __syncthreads();
@@ -443,12 +445,15 @@ __global__ void __launch_bounds__(256) mw_tc_prep_kernel(const float2* __restric
   }
 }
 
-// Device flag written by the tensor-core kernel when a bounded wait ran out.
+// Process-wide device flag: set (never cleared by a transform) whenever a
+// bounded wait of the tensor-core kernel ran out; ccfj_device_status reads
+// and clears it. Each call also has a flag of its own (MwTcDev::err), which
+// host-memory calls read, so overlapping calls never clear or inherit each
+// other's timeouts.
 __device__ unsigned int g_mw_tc_error = 0;
 
-int mw_tc_error(cudaStream_t s, bool* failed);
-
-int mwfj_tensor(const ccfj_eq_args& a, const float2* spec, cudaStream_t s, Scratch& sc) {
+int mwfj_tensor(const ccfj_eq_args& a, const float2* spec, cudaStream_t s, Scratch& sc,
+                unsigned int* call_err) {
   const int nr = a.ntr, nf = a.nf, nwin = a.nwin;
   CCFJ_REQUIRE(nr >= 2 && nwin >= 1, "MWFJ tensor path: needs nr >= 2 and nwin >= 1");
   int N = 2 * nwin;
@@ -473,8 +478,10 @@ int mwfj_tensor(const ccfj_eq_args& a, const float2* spec, cudaStream_t s, Scrat
       spec, nr, nf, nwin, N, nchunks, drs, bch);
   count_launch();
   CCFJ_LAUNCH_CHECK("mw_tc_prep_kernel");
-  unsigned int* err = nullptr;
-  CCFJ_CUDA_TRY(cudaGetSymbolAddress((void**)&err, g_mw_tc_error));
+  unsigned int* sticky = nullptr;
+  CCFJ_CUDA_TRY(cudaGetSymbolAddress((void**)&sticky, g_mw_tc_error));
+  unsigned int* err = call_err ? call_err : sc.get_n<unsigned int>(1);
+  if (!err) return CCFJ_ERR_ALLOC;
   CCFJ_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(unsigned int), s));
   MwTcDev d{};
   d.rs = a.r;
@@ -484,6 +491,7 @@ int mwfj_tensor(const ccfj_eq_args& a, const float2* spec, cudaStream_t s, Scrat
   d.c = a.c;
   d.out = a.out;
   d.err = err;
+  d.sticky = sticky;
   d.nr = nr;
   d.nf = nf;
   d.nc = a.nc;
@@ -523,10 +531,9 @@ int mw_tc_self_test(cudaStream_t s, int* status) {
   CCFJ_CUDA_TRY(cudaMemcpyAsync(fc, host_fc, sizeof(host_fc), cudaMemcpyHostToDevice, s));
   CCFJ_CUDA_TRY(cudaMemsetAsync(bch, 0, 2 * tc::kSlices * N * 32, s));
   float* wtr = sc.get_n<float>(nr);
-  if (!wtr) return CCFJ_ERR_ALLOC;
+  unsigned int* err = sc.get_n<unsigned int>(1);
+  if (!wtr || !err) return CCFJ_ERR_ALLOC;
   fj_prep_geom_kernel_shared(r, nr, drs, wtr, s);
-  unsigned int* err = nullptr;
-  CCFJ_CUDA_TRY(cudaGetSymbolAddress((void**)&err, g_mw_tc_error));
   CCFJ_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(unsigned int), s));
   MwTcDev d{};
   d.rs = r;
@@ -536,6 +543,7 @@ int mw_tc_self_test(cudaStream_t s, int* status) {
   d.c = fc + 1;
   d.out = out;
   d.err = err;
+  d.sticky = nullptr;  // the self-test's timeout is not a transform's
   d.nr = nr;
   d.nf = 1;
   d.nc = 1;
@@ -552,18 +560,26 @@ int mw_tc_self_test(cudaStream_t s, int* status) {
   count_launch();
   CCFJ_LAUNCH_CHECK("fj_mw_tc_kernel (self-test)");
   bool failed = false;
-  const int st = mw_tc_error(s, &failed);
+  const int st = mw_tc_call_error(err, s, &failed);
   if (st != CCFJ_OK) return st;
   *status = failed ? CCFJ_ERR_TIMEOUT : CCFJ_OK;
-  CCFJ_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(unsigned int), s));
-  CCFJ_CUDA_TRY(cudaStreamSynchronize(s));
   return CCFJ_OK;
 }
 
-int mw_tc_error(cudaStream_t s, bool* failed) {
+int mw_tc_call_error(const unsigned int* err, cudaStream_t s, bool* failed) {
   unsigned int h = 0;
+  CCFJ_CUDA_TRY(cudaMemcpyAsync(&h, err, sizeof(h), cudaMemcpyDeviceToHost, s));
+  CCFJ_CUDA_TRY(cudaStreamSynchronize(s));
+  *failed = h != 0;
+  return CCFJ_OK;
+}
+
+int mw_tc_sticky_error(cudaStream_t s, bool* failed) {
+  unsigned int h = 0;
+  const unsigned int zero = 0;
   CCFJ_CUDA_TRY(cudaMemcpyFromSymbolAsync(&h, g_mw_tc_error, sizeof(h), 0, cudaMemcpyDeviceToHost, s));
   CCFJ_CUDA_TRY(cudaStreamSynchronize(s));
+  if (h) CCFJ_CUDA_TRY(cudaMemcpyToSymbol(g_mw_tc_error, &zero, sizeof(zero)));
   *failed = h != 0;
   return CCFJ_OK;
 }

@@ -890,67 +890,6 @@ CCFJ_API int FH(float* u_f, float* r, float* f, float* out, float* c, int nc, in
   return ccfj::compat(u_f, r, f, out, c, nc, nr, nf, type, CCFJ_MODE_Y);
 }
 
-namespace ccfj {
-__global__ void special_device_kernel(int precision, long long n, const double* __restrict__ x,
-                                      double* __restrict__ out) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  double* o = out + 6 * i;
-  const double t = x[i] / fjs::kTwoPi;
-  if (precision == CCFJ_PREC_FP32) {
-    const float p_hi = (float)t;
-    const float p_lo = (float)(t - (double)p_hi);
-    fjs::ZB<float> J, Y;
-    fjs::eval_station_f32<true, true, true>((float)x[i], p_hi, p_lo, true, J, Y);
-    o[0] = J.z0; o[1] = J.z1; o[2] = J.b; o[3] = Y.z0; o[4] = Y.z1; o[5] = Y.b;
-  } else {
-    fjs::ZB<double> J, Y;
-    fjs::eval_station_f64<true, true, true>(x[i], t, J, Y);
-    o[0] = J.z0; o[1] = J.z1; o[2] = J.b; o[3] = Y.z0; o[4] = Y.z1; o[5] = Y.b;
-  }
-}
-}  // namespace ccfj
-
-CCFJ_API int ccfj_special_device(int precision, long long n, const double* x, double* out,
-                                 void* stream) {
-  ccfj::clear_error();
-  if (n < 0 || (n > 0 && (!x || !out)))
-    return ccfj::set_error(CCFJ_ERR_INVALID, "ccfj_special_device: bad arguments");
-  if (precision != CCFJ_PREC_FP32 && precision != CCFJ_PREC_FP64)
-    return ccfj::set_error(CCFJ_ERR_INVALID, "ccfj_special_device: bad precision %d", precision);
-  if (n == 0) return CCFJ_OK;
-  ccfj::special_device_kernel<<<ccfj::div_up(n, 256), 256, 0, (cudaStream_t)stream>>>(precision, n,
-                                                                                       x, out);
-  ccfj::count_launch();
-  CCFJ_LAUNCH_CHECK("special_device_kernel");
-  return CCFJ_OK;
-}
-
-CCFJ_API int ccfj_special_host(int precision, long long n, const double* x, double* out) {
-  ccfj::clear_error();
-  if (n < 0 || (n > 0 && (!x || !out)))
-    return ccfj::set_error(CCFJ_ERR_INVALID, "ccfj_special_host: bad arguments");
-  if (precision != CCFJ_PREC_FP32 && precision != CCFJ_PREC_FP64)
-    return ccfj::set_error(CCFJ_ERR_INVALID, "ccfj_special_host: bad precision %d", precision);
-  for (long long i = 0; i < n; ++i) {
-    double* o = out + 6 * i;
-    if (precision == CCFJ_PREC_FP32) {
-      // the phase in cycles as a double-float, as the kernels form it
-      const double t = x[i] / fjs::kTwoPi;
-      const float p_hi = (float)t;
-      const float p_lo = (float)(t - (double)p_hi);
-      fjs::ZB<float> J, Y;
-      fjs::eval_station_f32<true, true, true>((float)x[i], p_hi, p_lo, true, J, Y);
-      o[0] = J.z0; o[1] = J.z1; o[2] = J.b; o[3] = Y.z0; o[4] = Y.z1; o[5] = Y.b;
-    } else {
-      fjs::ZB<double> J, Y;
-      fjs::eval_station_f64<true, true, true>(x[i], x[i] / fjs::kTwoPi, J, Y);
-      o[0] = J.z0; o[1] = J.z1; o[2] = J.b; o[3] = Y.z0; o[4] = Y.z1; o[5] = Y.b;
-    }
-  }
-  return CCFJ_OK;
-}
-
 // --------------------------------------------------- allocation-free entry
 // ccfj_fj_noalloc_v1 runs the same FP32 transform as ccfj_fj_v1 with device
 // pointers, but takes its scratch (pair geometry and the per-interval

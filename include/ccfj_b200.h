@@ -112,7 +112,11 @@ CCFJ_API int ccfj_fj_v1(const ccfj_fj_args *args, void *stream);
  *     argument set into a CUDA graph and replayed on later calls (device
  *     mode; ignored when the stream is already being captured by the
  *     caller, or when a caller allocator is installed). The library keeps
- *     the 16 most recently launched graphs and destroys older ones.
+ *     the 16 most recently launched graphs and destroys older ones. With
+ *     stream NULL (the legacy default stream, which cannot capture) the
+ *     graph runs on a library stream that events order after the caller's
+ *     earlier default-stream work and before its later default-stream
+ *     work, as a launch on stream 0 would be.
  *   variant: velocities per thread, 1, 2 or 4 (0 = the choice recorded by
  *     ccfj_autotune_batch_v1 for the batch's class, else the untuned
  *     per-mode default described at ccfj_set_fj_variant).
@@ -166,15 +170,21 @@ CCFJ_API int ccfj_autotune_batch_v1(const ccfj_batch_args *args, void *stream,
  * output; the call itself allocates nothing (no cudaMalloc, cudaFree or
  * allocating library routine).
  *
- * Its scratch is one fixed 16 MiB array in the library's device image, which
- * every GPU that loads the library holds until the process exits. It fits
- * 24 * nr (+ 4 * nf for itype 1) plus, per input, 16 bytes (itype 1) or 4
- * bytes (itype 0) per (pair, frequency): about nr * nf <= 1.04e6 for one
- * itype-1 input. Larger problems are rejected with CCFJ_ERR_INVALID and a
- * message giving both sizes.
+ * Its scratch is one fixed 16 MiB array in the library's device image. A GPU
+ * holds it from the moment the CUDA runtime loads the code module that
+ * contains it onto that GPU until the process exits. Under lazy module
+ * loading (CUDA_MODULE_LOADING=LAZY, the default since CUDA 12.2) that moment
+ * is this entry point's first call on the device (or the first launch of a
+ * kernel of the same file), so that first call itself reserves the 16 MiB.
+ * It fits 24 * nr (+ 4 * nf for itype 1) plus, per input, 16 bytes (itype 1)
+ * or 4 bytes (itype 0) per (pair, frequency): about nr * nf <= 1.04e6 for
+ * one itype-1 input. Larger problems are rejected with CCFJ_ERR_INVALID and
+ * a message giving both sizes.
  *
- * The first call on each device looks up the array's device address with
- * that device current; make that first call before any stream capture.
+ * The first call on each device also looks up the array's device address
+ * with that device current. Make that first call -- a warm-up call on a
+ * small problem will do -- on every device before handing the free device
+ * memory to your own pool allocator, and before any stream capture.
  * Every call uses the same array and leaves its contents behind (each call
  * writes all the scratch it reads, so nothing is cleared): calls whose work
  * overlaps on the GPU -- on different streams, or from different threads --
@@ -223,8 +233,11 @@ CCFJ_API int ccfj_fj_earthquake_v1(const ccfj_eq_args *args, void *stream);
  * wherever supported. */
 CCFJ_API int ccfj_set_mwfj_path(int path);
 /* Waits for `stream` and reports CCFJ_ERR_TIMEOUT if a bounded device-side
- * wait of a tensor-core kernel ran out since the last such launch (host-
- * memory calls check this themselves). */
+ * wait of a tensor-core kernel ran out, in any call on this device, since
+ * the previous ccfj_device_status (which clears the record). Host-memory
+ * calls check their own kernels' waits through a flag of their own, so
+ * calls that overlap on different streams or threads neither clear nor
+ * inherit each other's timeouts. */
 CCFJ_API int ccfj_device_status(void *stream);
 /* Self-test of the bounded waits: runs one CTA of the tensor-core MWFJ
  * kernel whose input copy is never issued, with a ~1 ms wait limit, and
@@ -337,15 +350,5 @@ CCFJ_API int ccfj_fp32_peak_probe(void *stream, double *tflops);
 typedef void *(*ccfj_alloc_fn)(size_t bytes, void *stream, void *user);
 typedef void (*ccfj_free_fn)(void *ptr, void *stream, void *user);
 CCFJ_API int ccfj_set_allocator(ccfj_alloc_fn alloc, ccfj_free_fn free_fn, void *user);
-
-/* Host-side evaluation of the same special-function code the kernels use
- * (for unit tests of the approximations on machines without a GPU).
- * precision: CCFJ_PREC_FP32 or CCFJ_PREC_FP64. For each x[i] >= 0 writes
- * out[6*i .. 6*i+5] = J0, J1, BJ, Y0, Y1, BY with BZ(x) = int_0^x Z0. */
-CCFJ_API int ccfj_special_host(int precision, long long n, const double *x, double *out);
-/* The same on the device (x, out device pointers, async on stream): the
- * kernels' own instruction sequences, fast sine/cosine included. */
-CCFJ_API int ccfj_special_device(int precision, long long n, const double *x, double *out,
-                                 void *stream);
 
 #endif /* CCFJ_B200_H */

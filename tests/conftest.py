@@ -26,3 +26,10 @@ def golden():
 def lib():
     from ccfj import _lib
     return _lib.load()
+
+
+@pytest.fixture(scope="session")
+def probe():
+    """The test-only special-function probe library (not the product)."""
+    from ccfj import _lib
+    return _lib.load_probe()

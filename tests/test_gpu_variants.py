@@ -28,10 +28,14 @@ def _err(y, ref):
 
 @pytest.mark.parametrize("itype", [0, 1])
 @pytest.mark.parametrize("func", [0, 1])
-def test_single_set_variants_agree(lib, itype, func):
+@pytest.mark.parametrize("nc", [None, 37])
+def test_single_set_variants_agree(lib, itype, func, nc):
+    """nc = 37 leaves a partial velocity tile for every variant (37 is not a
+    multiple of 8 rows x 1, 2 or 4 velocities per thread)."""
     import ccfj
     case = cases.noise_case("noise_small")
-    args = (case["uf"], case["r"], case["c"], case["f"])
+    c = case["c"] if nc is None else np.linspace(900.0, 4800.0, nc)
+    args = (case["uf"], case["r"], c, case["f"])
     with warnings.catch_warnings():
         warnings.simplefilter("ignore")
         base = ccfj.fj_noise(*args, itype=itype, func=func)
@@ -66,8 +70,6 @@ def _device_batch(torch):
     T = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in dict(
         u=U.view(np.float32), off=off, perm=perm, r=rsorted, f=f.astype(np.float32),
         c=c.astype(np.float32)).items()}
-    # a graph launch with the null stream runs on a non-blocking library
-    # stream: the inputs must be on the device before the first call
     torch.cuda.synchronize()
 
     def args(out, use_graph=0, variant=0):
@@ -99,6 +101,35 @@ def test_batch_graph_cache_evicts_and_recaptures(lib):
         torch.cuda.synchronize()
         for o in outs:
             assert np.array_equal(o.cpu().numpy(), ref, equal_nan=True)
+    finally:
+        torch.cuda.synchronize()
+        assert lib.ccfj_batch_graph_cache_clear() == 0
+
+
+def test_batch_graph_null_stream_is_ordered(lib):
+    """A graph replay requested on the legacy default stream (NULL) runs
+    after the default-stream work queued before the call and before the
+    work queued after it, with no host synchronisation in between."""
+    import torch
+    from ccfj import _lib
+    assert torch.cuda.current_stream().cuda_stream == 0
+    args, ref, T = _device_batch(torch)
+    out = torch.empty(ref.shape, device="cuda")
+    try:
+        _lib.check(lib.ccfj_fj_batch_v1(ctypes.byref(args(out, use_graph=1)), None))  # capture
+        torch.cuda.synchronize()
+        u_true = T["u"].clone()
+        T["u"].zero_()
+        out.fill_(float("nan"))
+        torch.cuda.synchronize()
+        for _ in range(3):
+            torch.cuda._sleep(20_000_000)        # default stream busy for several ms
+            T["u"].copy_(u_true)                 # the inputs arrive only after that
+            _lib.check(lib.ccfj_fj_batch_v1(ctypes.byref(args(out, use_graph=1)), None))
+            got = out.clone()                    # default-stream work after the call
+            T["u"].zero_()
+            torch.cuda.synchronize()
+            assert np.array_equal(got.cpu().numpy(), ref, equal_nan=True)
     finally:
         torch.cuda.synchronize()
         assert lib.ccfj_batch_graph_cache_clear() == 0

@@ -10,21 +10,40 @@ import pytest
 from conftest import REPO
 
 
-def declared_symbols():
-    text = open(os.path.join(REPO, "include", "ccfj_b200.h")).read()
-    return re.findall(r"CCFJ_API\s+[\w\s\*]+?\b(\w+)\s*\(", text)
+def declared_symbols(header="ccfj_b200.h", macro="CCFJ_API"):
+    text = open(os.path.join(REPO, "include", header)).read()
+    return re.findall(macro + r"\s+[\w\s\*]+?\b(\w+)\s*\(", text)
 
 
 def test_header_declares_entry_points():
     syms = declared_symbols()
     for name in ("FJ", "FHr", "FHi", "FH", "ccfj_fj_v1", "ccfj_fj_earthquake_v1",
-                 "ccfj_last_error", "ccfj_set_allocator", "ccfj_special_host"):
+                 "ccfj_last_error", "ccfj_set_allocator", "ccfj_fj_noalloc_v1"):
         assert name in syms
 
 
 def test_library_exports_every_declared_symbol(lib):
     for name in declared_symbols():
         assert hasattr(lib, name), name
+
+
+def test_probe_library_is_separate(lib, probe):
+    """The special-function probes live in the test library only."""
+    syms = declared_symbols("ccfj_b200_probe.h", "CCFJ_PROBE_API")
+    assert set(syms) == {"ccfj_special_host", "ccfj_special_device"}
+    for name in syms:
+        assert hasattr(probe, name), name
+    import subprocess
+    from ccfj import _build
+    dyn = subprocess.run(["nm", "-D", "--defined-only", _build.LIB], capture_output=True,
+                         text=True).stdout
+    assert "ccfj_special_host" not in dyn and "ccfj_special_device" not in dyn
+
+
+def test_library_digest_matches_sources():
+    """The loaded library was built from the sources in this tree."""
+    from ccfj import _build
+    assert _build.up_to_date()
 
 
 def test_version(lib):

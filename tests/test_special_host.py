@@ -1,5 +1,5 @@
 """The special-function approximations of the kernels (host-compiled copy of
-the same source) against mpmath: J0, J1, Y0, Y1 and B = int_0^x Z0."""
+the same source, from the test library libccfj_b200_probe.so) against mpmath: J0, J1, Y0, Y1 and B = int_0^x Z0."""
 import ctypes
 
 import mpmath as mp
@@ -36,8 +36,8 @@ def _amplitude(x):
     return np.minimum(1.0, np.sqrt(2 / (np.pi * np.maximum(x, 1e-30))))
 
 
-def test_fp32_functions(lib):
-    got = _eval(lib, 0)
+def test_fp32_functions(probe):
+    got = _eval(probe, 0)
     amp = _amplitude(XS)
     for j, name in enumerate(("J0", "J1", "BJ", "Y0", "Y1", "BY")):
         scale = amp if name[0] != "B" else np.maximum(amp, np.abs(REF[:, j]))
@@ -47,8 +47,8 @@ def test_fp32_functions(lib):
         assert err.max() < 1.5e-6, (name, err.max(), XS[err.argmax()])
 
 
-def test_fp64_functions(lib):
-    got = _eval(lib, 1)
+def test_fp64_functions(probe):
+    got = _eval(probe, 1)
     amp = _amplitude(XS)
     for j, name in enumerate(("J0", "J1", "BJ", "Y0", "Y1", "BY")):
         scale = np.maximum(amp, np.abs(REF[:, j]))
@@ -58,21 +58,21 @@ def test_fp64_functions(lib):
         assert err.max() < 1.0, (name, err.max(), XS[err.argmax()])
 
 
-def test_bad_precision(lib):
+def test_bad_precision(probe):
     x = np.ones(1)
     out = np.zeros(6)
-    assert lib.ccfj_special_host(2, 1, x.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+    assert probe.ccfj_special_host(2, 1, x.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
                                  out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))) == 1
 
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("prec,tol", [(0, 1.5e-6), (1, None)])
-def test_device_functions(lib, prec, tol):
+def test_device_functions(probe, prec, tol):
     """The kernels' own code on the GPU (fast SFU sine/cosine in FP32)."""
     import torch
     x = torch.from_numpy(XS).cuda()
     out = torch.zeros((len(XS), 6), dtype=torch.float64, device="cuda")
-    st = lib.ccfj_special_device(prec, len(XS), ctypes.c_void_p(x.data_ptr()),
+    st = probe.ccfj_special_device(prec, len(XS), ctypes.c_void_p(x.data_ptr()),
                                  ctypes.c_void_p(out.data_ptr()), None)
     assert st == 0
     torch.cuda.synchronize()
