@@ -52,6 +52,15 @@ _lib.SIGNATURES["ccfj_autotune_batch_v1"] = (ctypes.c_int, [ctypes.POINTER(Batch
                                                              ctypes.POINTER(ctypes.c_float)])
 
 
+def _consecutive_complex64(parts):
+    """True when every part is a C-contiguous complex64 block that starts
+    right where the previous one ends in memory."""
+    if not all(p.dtype == np.complex64 and p.flags.c_contiguous for p in parts):
+        return False
+    return all(parts[b + 1].ctypes.data == parts[b].ctypes.data + parts[b].nbytes
+               for b in range(len(parts) - 1))
+
+
 def fj_noise_batch(ufs, rs, c, f, fstride=1, itype=1, func=0, variant=0):
     """fj_noise on every (uf_b, r_b) of the lists `ufs`, `rs` (shared c and
     f) in one launch. Each uf_b is [npairs_b, nf*fstride] (real part used).
@@ -83,14 +92,20 @@ def fj_noise_batch(ufs, rs, c, f, fstride=1, itype=1, func=0, variant=0):
     with warnings.catch_warnings():
         warnings.simplefilter("ignore", np.exceptions.ComplexWarning)
         parts = [np.asarray(u) for u in ufs]
-        if all(p.dtype == np.complex64 for p in parts):
+        for b, p in enumerate(parts):
+            if p.ndim != 2 or p.shape[0] != counts[b] or p.shape[1] != ncols:
+                raise ValueError("every uf_b must be [len(r_b), %d]" % ncols)
+        if _consecutive_complex64(parts):
+            # the subarrays are consecutive rows of one complex64 array (for
+            # example views of a pinned buffer): read them in place
+            U = parts
+            base_ptr, ld, es = parts[0].ctypes.data, 2 * ncols, 2
+        elif all(p.dtype == np.complex64 for p in parts):
             U = np.concatenate(parts, axis=0)
-            base, ld, es = U.view(np.float32), 2 * ncols, 2
+            base_ptr, ld, es = U.ctypes.data, 2 * ncols, 2
         else:
             U = np.concatenate([np.real(p).astype(np.float32) for p in parts], axis=0)
-            base, ld, es = U, ncols, 1
-    if U.shape[0] != offsets[-1] or U.shape[1] != ncols:
-        raise ValueError("every uf_b must be [len(r_b), %d]" % ncols)
+            base_ptr, ld, es = U.ctypes.data, ncols, 1
     f32 = np.ascontiguousarray(f, dtype=np.float32)
     c32 = np.ascontiguousarray(c, dtype=np.float32)
     out = np.empty((nsets, nc, nf), dtype=np.float32)
@@ -104,8 +119,8 @@ def fj_noise_batch(ufs, rs, c, f, fstride=1, itype=1, func=0, variant=0):
     a.use_graph, a.variant = 0, int(variant)
     a.offsets, a.total_pairs = offsets.ctypes.data, int(offsets[-1])
     a.r = rsorted.ctypes.data
-    a.u[0] = base.ctypes.data
-    a.u_ld, a.u_rows, a.u_es, a.u_ncols, a.fstride = ld, U.shape[0], es, ncols, fstride
+    a.u[0] = base_ptr
+    a.u_ld, a.u_rows, a.u_es, a.u_ncols, a.fstride = ld, int(offsets[-1]), es, ncols, fstride
     a.perm = perm.ctypes.data
     a.f, a.c, a.out = f32.ctypes.data, c32.ctypes.data, out.ctypes.data
     _lib.check(lib.ccfj_fj_batch_v1(ctypes.byref(a), None))

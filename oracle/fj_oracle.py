@@ -37,7 +37,8 @@ import scipy.special as sp
 from scipy import fftpack
 
 __all__ = ["struve_h01", "z_values", "fj_integral", "fj_integral_closed", "fj_trap", "fj_transform",
-           "fj_noise", "fj_earthquake", "MWFJ", "win", "hilbert_rows", "rel_error"]
+           "fj_noise", "fj_earthquake", "fj_earthquake_columns", "MWFJ", "mwfj_window_columns",
+           "win", "hilbert_rows", "rel_error"]
 
 _GL_X, _GL_W = np.polynomial.legendre.leggauss(6)
 DR_FLOOR = float(np.float32(0.1))  # fmaxf(r2 - r1, 0.1) in float32, src/FJcpu.cpp:259
@@ -270,6 +271,38 @@ def fj_earthquake(u, r, c, f, fstride=1, itype=1, func=0, normalize=True):
         outi = T(I, "J") + T(R, "Y")
     out = np.sqrt(outr ** 2 + outi ** 2)
     return _normalize(out) if normalize else out
+
+
+def fj_earthquake_columns(u, r, c, f, cols, itype=1, func=0):
+    """fj_earthquake (src/ccfj-gpu.pyx:270-295) restricted to the frequency
+    bins `cols` of f (fstride 1): the same rfft, the same float32 casts, the
+    transform of those columns only and their normalisation (every column
+    is independent of the others, so this equals the full call's columns).
+    Returns float64 [nc, len(cols)]."""
+    r, ufr, ufi = _eq_spectra(u, r, f, 1)
+    cols = np.asarray(cols)
+    fc = np.asarray(f)[cols]
+    R, r32, f32, c32 = _prep(ufr[:, cols], r, c, fc, 1)
+    I = _prep(ufi[:, cols], r, c, fc, 1)[0]
+    T = lambda X, basis: fj_transform(X, r32, f32, c32, itype, basis)  # noqa: E731
+    if func == 0:
+        outr, outi = T(R, "J"), T(I, "J")
+    else:
+        outr = T(R, "J") - T(I, "Y")
+        outi = T(I, "J") + T(R, "Y")
+    return _normalize(np.sqrt(outr ** 2 + outi ** 2))
+
+
+def mwfj_window_columns(u, r, c, f, Fs, winl_w, winr_w, cols, taper=0.9, itype=1, func=0):
+    """One window of MWFJ (src/ccfj-gpu.pyx:297-313): every trace j times
+    win(npts, Fs, winl_w[j], winr_w[j], taper), then fj_earthquake on the
+    bins `cols` (float64 [nc, len(cols)])."""
+    u = np.asarray(u)
+    nr, npts = len(r), u.shape[1]
+    u0 = np.zeros([nr, npts])
+    for j in range(nr):
+        u0[j, :] = u[j, :] * win(npts, Fs, winl_w[j], winr_w[j], taper)
+    return fj_earthquake_columns(u0, r, c, f, cols, itype, func)
 
 
 def win(npts, Fs, T1, T2, taper=0.8):
