@@ -45,6 +45,27 @@ __device__ __forceinline__ float taper_value(int t, const TaperSpec& w, int npts
   return (t < w.n1 || t >= tail) ? 0.0f : 1.0f;
 }
 
+// A sample range [lo, hi) outside which taper_value is zero: the hull of
+// the ramps [n1, n1 + delta), [n2 - delta, n2), [n2 + npts - delta,
+// n2 + npts) and the plateau [n1, tail), clipped to the trace. The FFT load
+// skips the samples outside it (a window of 200-2000 samples in a trace of
+// 16384 touches one eighth of the trace or less).
+__device__ __forceinline__ void taper_support(const TaperSpec& w, int npts, int& lo, int& hi) {
+  const int tail = w.n2 >= 0 ? w.n2 : max(npts + w.n2, 0);
+  const int s[4] = {w.n1, w.n2 - w.delta, w.n2 + npts - w.delta, w.n1};
+  const int e[4] = {w.n1 + w.delta, w.n2, w.n2 + npts, tail};
+  lo = npts;
+  hi = 0;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int a = max(s[j], 0), b = min(e[j], npts);
+    if (a < b) {
+      lo = min(lo, a);
+      hi = max(hi, b);
+    }
+  }
+}
+
 // Twiddles e^{-2 pi i t / M} for t < M/2, from FP64 sinpi/cospi.
 __global__ void fft_twiddle_kernel(int M, float2* __restrict__ tw) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -263,17 +284,29 @@ __global__ void __launch_bounds__(kStockMaxM / 16, 2)
   TaperSpec tp;
   if (taper) tp = job.taper[row];
   // first pass (radix 16, Ns = 1): z[m] = x[2m] + i x[2m+1], m = tid + r P
-  // all 16 loads are issued before any taper arithmetic, so they overlap
+  // all 16 loads are issued before any taper arithmetic, so they overlap;
+  // with a taper, points whose two samples lie outside the window's support
+  // are zero and are not loaded
   float2 v[16];
-#pragma unroll
-  for (int r = 0; r < 16; ++r) v[r] = __ldg(x + tid + r * P);
   if (taper) {
+    int lo, hi;
+    taper_support(tp, job.npts, lo, hi);
 #pragma unroll
     for (int r = 0; r < 16; ++r) {
       const int m = tid + r * P;
-      v[r].x *= taper_value(2 * m, tp, job.npts);
-      v[r].y *= taper_value(2 * m + 1, tp, job.npts);
+      v[r] = (2 * m + 1 >= lo && 2 * m < hi) ? __ldg(x + m) : make_float2(0.0f, 0.0f);
     }
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+      const int m = tid + r * P;
+      if (2 * m + 1 >= lo && 2 * m < hi) {
+        v[r].x *= taper_value(2 * m, tp, job.npts);
+        v[r].y *= taper_value(2 * m + 1, tp, job.npts);
+      }
+    }
+  } else {
+#pragma unroll
+    for (int r = 0; r < 16; ++r) v[r] = __ldg(x + tid + r * P);
   }
   stockham_fft(v, sz, M, tw, tid, P);
   // real-transform split, bins k < nbins (k <= M)

@@ -24,10 +24,13 @@ What it restates (reference file:line):
     - pair (a, b) gets conj(X_a) X_b added when both take part, and a count
       (:118-131); each pair with a nonzero count is divided by it (:133-144).
 
-FFTW is not in this image, so src/CrossCorr.cpp cannot be built here and
-the reference's cross-correlator has not been run: parity unpinned. The
-restatement is checked against properties that follow from the code above
-(tests/test_cc_oracle.py).
+Pinning: FFTW is not in this image, so src/CrossCorr.cpp is compiled
+unmodified against oracle/fftw_shim (this project's FP64 stand-in for the
+few FFTW calls it makes) into oracle/_ref, and tests/golden/
+make_cc_golden.py records the reference's CC outputs on six seeded cases
+(tests/golden/cc_reference_outputs.npz). tests/test_cc_golden.py holds
+this restatement to them within 2e-5 of each pair's largest value;
+tests/test_cc_oracle.py adds properties that follow from the code above.
 
 Arithmetic: float64 on the float32 (one-bit: sign) samples with numpy's
 rfft; the reference works in float32 with FFTW.

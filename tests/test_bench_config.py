@@ -44,3 +44,66 @@ def test_config_names_the_workload():
                                                                                  1, 0)
     assert "workload" in cfg and "l2" in cfg
     assert os.path.exists(os.path.join(REPO, "bench.py"))
+
+
+def _ref_module():
+    import pytest
+    bench = _bench()
+    try:
+        return bench, bench.reference_module()
+    except ImportError:
+        pytest.skip("the reference's CPU build (make -C oracle) is not present")
+
+
+def test_reference_column_samples_equal_full_calls():
+    """The CPU baseline's column samples reproduce the reference's own full
+    calls on those columns: fj_noise, fj_earthquake and one MWFJ window."""
+    import cases
+    bench, ref = _ref_module()
+    import warnings
+    warnings.simplefilter("ignore")
+    n = cases.noise_case("noise_small")
+    full = ref.fj_noise(n["uf"], n["r"], n["c"], n["f"], num=2)
+    cols = np.array([3, 9, 30])
+    _, o = bench.ref_noise_cols(ref, n["uf"], n["r"], n["c"], n["f"], cols, 2)
+    assert np.array_equal(o, full[:, cols], equal_nan=True)
+    e = cases.eq_case("eq_small")
+    full = ref.fj_earthquake(e["u"], e["r"], e["c"], e["f"], num=2)
+    cols = np.array([0, 5, 17, 39])                      # bin 0: the NaN column
+    _, _, o = bench.ref_eq_cols(ref, e["u"], e["r"], e["c"], e["f"], cols, 2)
+    assert np.array_equal(o, full[:, cols], equal_nan=True)
+    m = cases.mwfj_case("mwfj_small")
+    full = ref.MWFJ(m["u"], m["r"], m["c"], m["f"], m["Fs"], m["nwin"], m["winl"], m["winr"],
+                    m["taper"], num=2)
+    wl = {k: m[k] for k in ("u", "r", "c", "f", "Fs", "winl", "winr", "taper")}
+    cols = np.array([1, 7, 20])
+    _, _, o = bench.ref_mwfj_window_cols(ref, wl, 2, cols, 2)
+    assert np.allclose(o, full[2][:, cols], rtol=0, atol=0)
+
+
+def test_column_sets_cover_the_band_evenly():
+    bench = _bench()
+    sets = bench.column_sets(2048, 16, 20)
+    allc = np.sort(np.concatenate(sets))
+    assert len(sets) == 20 and all(len(s) == 16 for s in sets)
+    assert len(np.unique(allc)) == 320 and allc[0] == 0 and allc[-1] == 2047
+    gaps = np.diff(allc)
+    assert gaps.max() - gaps.min() <= 1                  # evenly spaced
+    for s in sets:                                      # each step spans the band
+        assert s.min() < 128 and s.max() > 1900
+
+
+def test_oracle_column_helpers_equal_full_oracle():
+    import cases
+    import fj_oracle as O
+    e = cases.eq_case("eq_small")
+    full = O.fj_earthquake(e["u"], e["r"], e["c"], e["f"])
+    cols = [0, 3, 17, 39]
+    sub = O.fj_earthquake_columns(e["u"], e["r"], e["c"], e["f"], cols)
+    assert np.array_equal(sub, full[:, cols], equal_nan=True)
+    m = cases.mwfj_case("mwfj_small")
+    full = O.MWFJ(m["u"], m["r"], m["c"], m["f"], m["Fs"], m["nwin"], m["winl"], m["winr"],
+                  m["taper"])
+    sub = O.mwfj_window_columns(m["u"], m["r"], m["c"], m["f"], m["Fs"], m["winl"][1],
+                                m["winr"][1], [2, 5, 9], m["taper"])
+    assert np.array_equal(sub, full[1][:, [2, 5, 9]], equal_nan=True)

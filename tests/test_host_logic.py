@@ -115,3 +115,42 @@ def test_fj_noise_argument_errors_before_device_work(capsys):
             ccfj.fj_noise(case["uf"][:, :-1], case["r"], case["c"], case["f"])
         with pytest.raises(ValueError):
             ccfj.fj_noise(case["uf"], case["r"], case["c"], case["f"], fstride=0)
+
+
+def _device_support(npts, n1, n2, dl):
+    """taper_support in fj_fft.cu, restated: the hull of the ramps and the
+    plateau, clipped to [0, npts)."""
+    tail = n2 if n2 >= 0 else max(npts + n2, 0)
+    lo, hi = npts, 0
+    for s, e in ((n1, n1 + dl), (n2 - dl, n2), (n2 + npts - dl, n2 + npts), (n1, tail)):
+        a, b = max(s, 0), min(e, npts)
+        if a < b:
+            lo, hi = min(lo, a), max(hi, b)
+    return lo, hi
+
+
+def test_device_taper_support_holds_every_nonzero_sample():
+    """The FFT front end loads no sample outside taper_support's range; the
+    taper is zero there for every window the device can receive (the same
+    600+ windows, plus the configuration-4 window shapes)."""
+    from ccfj import _eq
+    rng = np.random.default_rng(19)
+    wins = _windows() + [(int(rng.integers(4, 200)), float(rng.choice([1.0, 2.0, 0.5])),
+                          float(rng.uniform(-50, 300)), float(rng.uniform(-300, 300)),
+                          float(rng.uniform(-3, 3))) for _ in range(600)]
+    L = rng.integers(200, 2001, size=50)
+    start = rng.integers(0, 16384 - L)
+    wins += [(16384, 10.0, s / 10.0, (s + n) / 10.0, 0.9) for s, n in zip(start, L)]
+    checked = 0
+    for npts, Fs, T1, T2, taper in wins:
+        params, perr = _call(_eq._win_params, npts, Fs, [T1], [T2], taper)
+        if perr is not None:
+            continue
+        n1, n2, dl = (int(v[0]) for v in params)
+        w = _device_rule(npts, n1, n2, dl)
+        lo, hi = _device_support(npts, n1, n2, dl)
+        outside = np.ones(npts, dtype=bool)
+        outside[lo:hi] = False
+        assert not np.any(w[outside] != 0), (npts, Fs, T1, T2, taper, lo, hi)
+        checked += 1
+    assert checked > 500
