@@ -137,3 +137,54 @@ def CC(npts, nsta, nf, fftlen, Pairs, startend, data, overlaprate=0.0, nThreads=
                              fstride, ifonebit, ifspecwhittenning)
     _lib.check(_lib.load().ccfj_cc_v1(ctypes.byref(a), None))
     return out
+
+
+_lib.SIGNATURES["ccfj_cc_fj_noise_v1"] = (ctypes.c_int, [ctypes.POINTER(CcArgs),
+                                                          ctypes.POINTER(_lib.FjArgs),
+                                                          ctypes.c_void_p])
+
+
+def cc_fj_noise(npts, nsta, nf, fftlen, Pairs, startend, data, r, c, f, overlaprate=0.0,
+                fstride=1, ifonebit=0, ifspecwhittenning=1, itype=1, func=0):
+    """Records to a normalised F-J dispersion spectrum in one call: the
+    reference's pipeline CC(...) followed by fj_noise(ncfs, r, c, f, itype,
+    func) (examples/example_noise.py:6-11), with the cross-spectra kept on
+    the device between the two steps. The records cross to the device once
+    and the float32 [nc, nf] spectrum comes back once.
+
+    The CC arguments are those of `CC` (one-bit is applied to the samples as
+    they are read: `data` is not rewritten, unlike CC); r [npairs] holds the
+    distance of each pair of Pairs, f the nf frequencies of the bins
+    j*fstride, c the velocities; itype and func as in fj_noise (func 1 takes
+    the Hilbert transform of each pair's spectrum along frequency)."""
+    if func not in (0, 1):
+        raise ValueError("func must be 0 (Bessel) or 1 (Hankel), got %r" % (func,))
+    if itype not in (0, 1):
+        raise ValueError("itype must be 0 or 1, got %r" % (itype,))
+    a, keep, _ = _prepare(npts, nsta, nf, fftlen, Pairs, startend, data, overlaprate, fstride,
+                          ifonebit, ifspecwhittenning)
+    npairs = a.npairs
+    r = np.asarray(r)
+    if r.shape != (npairs,):
+        raise ValueError("r must hold one distance per pair (%d), got shape %s"
+                         % (npairs, r.shape))
+    if len(f) != nf:
+        raise ValueError("f must hold the nf=%d frequencies of the bins" % nf)
+    indx = np.argsort(r)
+    perm = np.ascontiguousarray(indx, dtype=np.int64)
+    rs = np.ascontiguousarray(r[indx], dtype=np.float32)
+    f32 = np.ascontiguousarray(f, dtype=np.float32)
+    c32 = np.ascontiguousarray(c, dtype=np.float32)
+    out = np.empty((len(c), nf), dtype=np.float32)
+    fa = _lib.FjArgs()
+    fa.struct_size = ctypes.sizeof(_lib.FjArgs)
+    fa.nr, fa.nf, fa.nc = npairs, nf, len(c)
+    fa.itype = int(itype)
+    fa.mode = _lib.MODE_J if func == 0 else _lib.MODE_J_MINUS_Y
+    fa.precision, fa.normalize, fa.device_ptrs = _lib.PREC_FP32, 1, 0
+    fa.perm, fa.r, fa.f, fa.c = perm.ctypes.data, rs.ctypes.data, f32.ctypes.data, c32.ctypes.data
+    fa.out = out.ctypes.data
+    a.out_re = None
+    _lib.check(_lib.load().ccfj_cc_fj_noise_v1(ctypes.byref(a), ctypes.byref(fa), None))
+    del keep  # the records, pairs and ranges the call read
+    return out

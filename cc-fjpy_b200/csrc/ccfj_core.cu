@@ -139,3 +139,25 @@ CCFJ_API int ccfj_set_allocator(ccfj_alloc_fn alloc, ccfj_free_fn free_fn, void*
   ccfj::g_alloc_user = user;
   return CCFJ_OK;
 }
+
+CCFJ_API int ccfj_host_alloc(size_t bytes, void** ptr) {
+  ccfj::clear_error();
+  if (!ptr) return ccfj::set_error(CCFJ_ERR_INVALID, "ccfj_host_alloc: ptr is NULL");
+  *ptr = nullptr;
+  const cudaError_t e = cudaHostAlloc(ptr, bytes ? bytes : 1, cudaHostAllocPortable);
+  if (e != cudaSuccess) {
+    *ptr = nullptr;
+    return ccfj::set_error(CCFJ_ERR_ALLOC, "ccfj_host_alloc: cudaHostAlloc(%zu) failed: %s", bytes,
+                           cudaGetErrorString(e));
+  }
+  return CCFJ_OK;
+}
+
+CCFJ_API int ccfj_host_free(void* ptr) {
+  ccfj::clear_error();
+  if (!ptr) return CCFJ_OK;
+  const cudaError_t e = cudaFreeHost(ptr);
+  if (e != cudaSuccess)
+    return ccfj::set_error(CCFJ_ERR_CUDA, "ccfj_host_free: %s", cudaGetErrorString(e));
+  return CCFJ_OK;
+}

@@ -474,6 +474,8 @@ static int validate(const ccfj_fj_args* a) {
   return CCFJ_OK;
 }
 
+int fj_validate(const ccfj_fj_args* a) { return validate(a); }
+
 // ------------------------------------------ host memory, in frequency blocks
 // Frequency columns are independent (the per-frequency normalisation
 // included), so a large host-memory transform without the Hilbert transform

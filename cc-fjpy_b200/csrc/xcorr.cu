@@ -30,6 +30,7 @@
 #include "cc_core.cuh"
 #include "cc_plan.h"
 #include "ccfj_core.cuh"
+#include "fj_frontend.cuh"
 
 namespace ccfj {
 namespace xc {
@@ -385,8 +386,103 @@ static int run(const ccfj_cc_args& a, cudaStream_t s) {
   return CCFJ_OK;
 }
 
+// Records to dispersion spectrum: the cross-correlation writes its
+// complex64 cross-spectra into device scratch, and the transform reads
+// their real parts there (perm, r, f, c and out as the caller gives them).
+static int cc_fj_noise(const ccfj_cc_args& cc, const ccfj_fj_args& fj, cudaStream_t s) {
+  CCFJ_REQUIRE(cc.struct_size == (int)sizeof(ccfj_cc_args),
+               "ccfj_cc_fj_noise_v1: cc struct_size=%d, expected %d", cc.struct_size,
+               (int)sizeof(ccfj_cc_args));
+  CCFJ_REQUIRE(!cc.accumulate, "ccfj_cc_fj_noise_v1: cc->accumulate must be 0");
+  CCFJ_REQUIRE(cc.device_ptrs == fj.device_ptrs,
+               "ccfj_cc_fj_noise_v1: cc->device_ptrs (%d) != fj->device_ptrs (%d)",
+               cc.device_ptrs, fj.device_ptrs);
+  CCFJ_REQUIRE(cc.data != nullptr, "ccfj_cc_fj_noise_v1: data is NULL");
+  CCFJ_REQUIRE(fj.nr == cc.npairs && fj.nf == cc.nf,
+               "ccfj_cc_fj_noise_v1: fj nr=%d nf=%d must equal the pairs (%d) and bins (%d)",
+               fj.nr, fj.nf, cc.npairs, cc.nf);
+  CCFJ_REQUIRE(fj.mode == CCFJ_MODE_J || fj.mode == CCFJ_MODE_J_MINUS_Y,
+               "ccfj_cc_fj_noise_v1: mode must be CCFJ_MODE_J (func 0) or CCFJ_MODE_J_MINUS_Y "
+               "(func 1)");
+  CCFJ_REQUIRE(cc.npairs >= 1 && cc.nf >= 1, "ccfj_cc_fj_noise_v1: npairs=%d nf=%d", cc.npairs,
+               cc.nf);
+  Scratch sc(s);
+  float* spec = sc.get_n<float>(2 * (size_t)cc.npairs * cc.nf);
+  if (!spec) return CCFJ_ERR_ALLOC;
+  ccfj_cc_args c = cc;
+  c.device_ptrs = 1;
+  c.out_layout = 1;
+  c.out_re = spec;
+  c.out_im = nullptr;
+  const long long nrec = (long long)cc.nsta * cc.npts;
+  if (!cc.device_ptrs) {  // the records cross to the device once
+    CCFJ_REQUIRE(cc.nsta >= 1 && cc.npts >= 1, "ccfj_cc_fj_noise_v1: nsta=%d npts=%d", cc.nsta,
+                 cc.npts);
+    float* d = sc.get_n<float>(nrec);
+    if (!d) return CCFJ_ERR_ALLOC;
+    CCFJ_CUDA_TRY(cudaMemcpyAsync(d, cc.data, nrec * sizeof(float), cudaMemcpyHostToDevice, s));
+    c.data = d;
+  }
+  ccfj_fj_args f = fj;
+  f.u[0] = spec;
+  f.u[1] = nullptr;
+  f.u_ld = 2LL * cc.nf;
+  f.u_rows = cc.npairs;
+  f.u_es = 2;
+  f.u_ncols = cc.nf;
+  f.fstride = 1;
+  f.hilbert = fj.mode == CCFJ_MODE_J_MINUS_Y ? 1 : 0;
+  f.col_begin = 0;
+  f.nf_total = 0;
+  f.device_ptrs = 1;
+  int st = fj_validate(&f);
+  if (st != CCFJ_OK) return st;
+  if (!fj.device_ptrs) {  // the small per-pair and grid arrays, and the result
+    float* dr = sc.get_n<float>(fj.nr);
+    float* df = sc.get_n<float>(fj.nf);
+    float* dc = sc.get_n<float>(fj.nc);
+    float* dout = sc.get_n<float>((size_t)fj.nc * fj.nf);
+    long long* dp = fj.perm ? sc.get_n<long long>(fj.nr) : nullptr;
+    if (!dr || !df || !dc || !dout || (fj.perm && !dp)) return CCFJ_ERR_ALLOC;
+    if (fj.perm)
+      for (int i = 0; i < fj.nr; ++i)
+        CCFJ_REQUIRE(fj.perm[i] >= 0 && fj.perm[i] < fj.nr,
+                     "ccfj_cc_fj_noise_v1: perm[%d]=%lld out of range", i, fj.perm[i]);
+    CCFJ_CUDA_TRY(cudaMemcpyAsync(dr, fj.r, sizeof(float) * fj.nr, cudaMemcpyHostToDevice, s));
+    CCFJ_CUDA_TRY(cudaMemcpyAsync(df, fj.f, sizeof(float) * fj.nf, cudaMemcpyHostToDevice, s));
+    CCFJ_CUDA_TRY(cudaMemcpyAsync(dc, fj.c, sizeof(float) * fj.nc, cudaMemcpyHostToDevice, s));
+    if (dp)
+      CCFJ_CUDA_TRY(cudaMemcpyAsync(dp, fj.perm, sizeof(long long) * fj.nr, cudaMemcpyHostToDevice,
+                                    s));
+    f.r = dr;
+    f.f = df;
+    f.c = dc;
+    f.out = dout;
+    f.perm = dp;
+  }
+  st = run(c, s);
+  if (st != CCFJ_OK) return st;
+  st = fj_device(f, s);
+  if (st != CCFJ_OK) return st;
+  if (!fj.device_ptrs) {
+    CCFJ_CUDA_TRY(cudaMemcpyAsync(fj.out, f.out, sizeof(float) * fj.nc * fj.nf,
+                                  cudaMemcpyDeviceToHost, s));
+    CCFJ_CUDA_TRY(cudaStreamSynchronize(s));
+  }
+  return CCFJ_OK;
+}
+
 }  // namespace xc
 }  // namespace ccfj
+
+CCFJ_API int ccfj_cc_fj_noise_v1(const ccfj_cc_args* cc, const ccfj_fj_args* fj, void* stream) {
+  ccfj::clear_error();
+  if (!cc || !fj) return ccfj::set_error(CCFJ_ERR_INVALID, "ccfj_cc_fj_noise_v1: NULL args");
+  if (fj->struct_size != (int)sizeof(ccfj_fj_args))
+    return ccfj::set_error(CCFJ_ERR_INVALID, "ccfj_cc_fj_noise_v1: fj struct_size=%d, expected %d",
+                           fj->struct_size, (int)sizeof(ccfj_fj_args));
+  return ccfj::xc::cc_fj_noise(*cc, *fj, (cudaStream_t)stream);
+}
 
 CCFJ_API int ccfj_cc_v1(const ccfj_cc_args* args, void* stream) {
   ccfj::clear_error();

@@ -311,6 +311,29 @@ typedef struct ccfj_cc_data {
 
 CCFJ_API int CrossCorrelation(ccfj_cc_data data);
 
+/* ------------------------------------- records to dispersion spectrum
+ * The reference's ambient-noise pipeline, CC then fj_noise
+ * (examples/example_noise.py:6-11 over src/ccfj.pyx:125-147 and
+ * src/ccfj-gpu.pyx:241-268), in one call whose cross-spectra never leave the
+ * device: the cross-correlation writes them into device scratch and the
+ * transform reads their real parts there.
+ *   cc: as ccfj_cc_v1, with accumulate = 0; out_re, out_im and out_layout
+ *       are not used. Unlike CC, one-bit never rewrites cc->data (the
+ *       records are read, signed on load, and left as they were).
+ *   fj: as ccfj_fj_v1 for the transform of those spectra: nr = cc->npairs,
+ *       nf = cc->nf, mode CCFJ_MODE_J (fj_noise func 0) or
+ *       CCFJ_MODE_J_MINUS_Y (func 1: the Hilbert transform of each pair's
+ *       spectrum along frequency is taken on the device); u, u_ld, u_rows,
+ *       u_es, u_ncols, fstride, hilbert, col_begin and nf_total are set by
+ *       the call. perm (optional) maps sorted pair i to its row of the
+ *       cross-spectra, r is the sorted distances, f the nf frequencies of the
+ *       bins, c the velocities, out [nc][nf].
+ *   cc->device_ptrs must equal fj->device_ptrs. Host mode: the records cross
+ *   to the device once, the [nc][nf] result once back, and the call is
+ *   synchronous. No counterpart entry in the reference, which returns the
+ *   cross-spectra to the host between the two steps. */
+CCFJ_API int ccfj_cc_fj_noise_v1(const ccfj_cc_args *cc, const ccfj_fj_args *fj, void *stream);
+
 /* ------------------------------------------------------------- tuning
  * The FP32 kernels come in variants that give each thread 1, 2 or 4
  * velocities. ccfj_autotune_fj_v1 runs every variant on the given problem
@@ -350,5 +373,13 @@ CCFJ_API int ccfj_fp32_peak_probe(void *stream, double *tflops);
 typedef void *(*ccfj_alloc_fn)(size_t bytes, void *stream, void *user);
 typedef void (*ccfj_free_fn)(void *ptr, void *stream, void *user);
 CCFJ_API int ccfj_set_allocator(ccfj_alloc_fn alloc, ccfj_free_fn free_fn, void *user);
+
+/* Page-locked (pinned) host memory of `bytes` bytes, usable by every device
+ * (cudaHostAlloc, portable), and its release. Host arrays in pinned memory
+ * cross to the device by DMA without a staging copy; ccfj.load_ncfs reads
+ * stored cross-spectra straight into such a buffer. No counterpart in the
+ * reference. */
+CCFJ_API int ccfj_host_alloc(size_t bytes, void **ptr);
+CCFJ_API int ccfj_host_free(void *ptr);
 
 #endif /* CCFJ_B200_H */
