@@ -69,6 +69,10 @@ SIGNATURES = {
                                            ctypes.POINTER(ctypes.c_int),
                                            ctypes.POINTER(ctypes.c_float)]),
     "ccfj_set_fj_variant": (ctypes.c_int, [ctypes.c_int]),
+    "ccfj_set_fj_split": (ctypes.c_int, [ctypes.c_int]),
+    "ccfj_set_tune_cache": (ctypes.c_int, [ctypes.c_char_p]),
+    "ccfj_tuned_choice_fj": (ctypes.c_int, [ctypes.POINTER(FjArgs), ctypes.POINTER(ctypes.c_int),
+                                            ctypes.POINTER(ctypes.c_int)]),
     "ccfj_last_error": (ctypes.c_char_p, []),
     "ccfj_version": (ctypes.c_char_p, []),
     "ccfj_launch_count": (ctypes.c_longlong, []),

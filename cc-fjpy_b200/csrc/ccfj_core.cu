@@ -1,8 +1,13 @@
-// Host-side plumbing of the C-ABI: errors, allocator, launch counter.
+// Host-side plumbing of the C-ABI: errors, allocator, launch counter, the
+// autotuners' table.
 #include <atomic>
+#include <cstdlib>
+#include <map>
 #include <mutex>
+#include <utility>
 
 #include "ccfj_core.cuh"
+#include "tune_cache.h"
 
 namespace ccfj {
 
@@ -28,6 +33,84 @@ int set_error(int status, const char* fmt, ...) {
 void clear_error() { g_last_error.clear(); }
 
 void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+// ------------------------------------------------------ autotuner table
+// In-process choices of both autotuners, keyed by (tuner, class key, device
+// name), backed by the file named by ccfj_set_tune_cache or, by default,
+// the environment variable CCFJ_TUNE_CACHE (no file: in-process only). The
+// file is read on the first lookup of each device, and every tuning result
+// is written through to it.
+namespace {
+std::mutex g_tune_mu;
+std::map<std::pair<std::string, std::string>, int> g_tunes;  // (kind + device, key) -> choice
+std::map<std::string, bool> g_tune_loaded;                   // device -> read
+bool g_tune_path_set = false;
+std::string g_tune_path;
+
+// The current device's name token (queried once per device ordinal).
+std::string current_device_token() {
+  static std::mutex mu;
+  static std::map<int, std::string> names;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return tune::device_token("");
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = names.find(dev);
+  if (it != names.end()) return it->second;
+  cudaDeviceProp p{};
+  const std::string t =
+      tune::device_token(cudaGetDeviceProperties(&p, dev) == cudaSuccess ? p.name : "");
+  names[dev] = t;
+  return t;
+}
+
+std::string tune_path_locked() {
+  if (g_tune_path_set) return g_tune_path;
+  const char* env = std::getenv("CCFJ_TUNE_CACHE");
+  return env ? std::string(env) : std::string();
+}
+
+std::pair<std::string, std::string> tune_slot(const std::string& kind, const std::string& device,
+                                              long long key) {
+  return {kind + "|" + device, std::to_string(key)};
+}
+
+void tune_load_locked(const std::string& device) {
+  if (g_tune_loaded[device]) return;
+  g_tune_loaded[device] = true;
+  const std::string path = tune_path_locked();
+  if (path.empty()) return;
+  for (const tune::Entry& e : tune::read_file(path))
+    if (e.device == device) g_tunes[tune_slot(e.kind, e.device, e.key)] = e.choice;
+}
+}  // namespace
+
+bool tune_lookup(const char* kind, long long key, int* choice) {
+  const std::string device = current_device_token();
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  tune_load_locked(device);
+  auto it = g_tunes.find(tune_slot(kind, device, key));
+  if (it == g_tunes.end()) return false;
+  *choice = it->second;
+  return true;
+}
+
+int tune_record(const char* kind, long long key, int choice, float ms) {
+  const std::string device = current_device_token();
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  tune_load_locked(device);
+  g_tunes[tune_slot(kind, device, key)] = choice;
+  const std::string path = tune_path_locked();
+  if (path.empty()) return CCFJ_OK;
+  tune::Entry e;
+  e.device = device;
+  e.kind = kind;
+  e.key = key;
+  e.choice = choice;
+  e.ms = ms;
+  if (!tune::upsert_file(path, e))
+    return set_error(CCFJ_ERR_INVALID, "autotuner: cannot write the table %s", path.c_str());
+  return CCFJ_OK;
+}
 
 // Scratch comes from one stream-ordered memory pool per device that keeps
 // its memory between calls (release threshold = max): without it, every
@@ -159,5 +242,14 @@ CCFJ_API int ccfj_host_free(void* ptr) {
   const cudaError_t e = cudaFreeHost(ptr);
   if (e != cudaSuccess)
     return ccfj::set_error(CCFJ_ERR_CUDA, "ccfj_host_free: %s", cudaGetErrorString(e));
+  return CCFJ_OK;
+}
+
+CCFJ_API int ccfj_set_tune_cache(const char* path) {
+  ccfj::clear_error();
+  std::lock_guard<std::mutex> lk(ccfj::g_tune_mu);
+  ccfj::g_tune_path_set = path != nullptr;
+  ccfj::g_tune_path = path ? path : "";
+  ccfj::g_tune_loaded.clear();  // read the (new) table again on the next lookup
   return CCFJ_OK;
 }

@@ -74,6 +74,13 @@ class Scratch {
 void prof_begin(cudaStream_t s);
 void prof_end(cudaStream_t s);
 
+// The autotuners' table: the recorded choice of tuner `kind` ("fj",
+// "batch") for a problem class on the current device, and a new record
+// (written through to the persistent table when one is configured; the
+// status reports a failed write).
+bool tune_lookup(const char* kind, long long key, int* choice);
+int tune_record(const char* kind, long long key, int choice, float ms);
+
 // Counts kernel launches issued by this library (per process); the benchmark
 // reads it to report how many of its own kernels a step launched.
 void count_launch(int n = 1);

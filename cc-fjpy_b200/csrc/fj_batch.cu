@@ -265,8 +265,6 @@ int batch_validate(const ccfj_batch_args* a) {
 // itype and the powers of two of the total pairs, sets, nf and nc), as
 // recorded by ccfj_autotune_batch_v1; variant 0 uses it, else the untuned
 // per-mode default.
-std::mutex g_btune_mu;
-std::map<long long, int> g_btune;
 
 long long batch_tune_key(const ccfj_batch_args& a, long long total) {
   auto lg = [](long long v) {
@@ -280,9 +278,9 @@ long long batch_tune_key(const ccfj_batch_args& a, long long total) {
 
 int batch_variant(const ccfj_batch_args& a, long long total) {
   if (a.variant > 0) return a.variant;
-  std::lock_guard<std::mutex> lk(g_btune_mu);
-  auto it = g_btune.find(batch_tune_key(a, total));
-  return it == g_btune.end() ? default_cpt_for(a.mode, a.itype) : it->second;
+  int choice = 0;
+  return tune_lookup("batch", batch_tune_key(a, total), &choice) ? choice
+                                                                  : default_cpt_for(a.mode, a.itype);
 }
 
 // The device sequence of one batch (all pointers device pointers;
@@ -636,13 +634,10 @@ CCFJ_API int ccfj_autotune_batch_v1(const ccfj_batch_args* args, void* stream, i
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (st != CCFJ_OK) return st;
-  {
-    std::lock_guard<std::mutex> lk(ccfj::g_btune_mu);
-    ccfj::g_btune[ccfj::batch_tune_key(*args, args->total_pairs)] = best;
-  }
+  st = ccfj::tune_record("batch", ccfj::batch_tune_key(*args, args->total_pairs), best, best_t);
   if (best_variant) *best_variant = best;
   if (best_ms) *best_ms = best_t;
-  return CCFJ_OK;
+  return st;
 }
 
 CCFJ_API int ccfj_batch_graph_cache_clear(void) {

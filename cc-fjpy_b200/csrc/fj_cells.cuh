@@ -225,6 +225,13 @@ struct FjDev {
   float* out;
   int nr, nf, nc;
   float tau;
+  // Station range [i_lo, i_hi) of this launch (the whole set: 0, nr). With
+  // `part` set, the raw sums of the range (before the amplitude gamma and
+  // the magnitude) go to part[q][nc][nf] (q < the mode's accumulators)
+  // instead of out, for a later fixed-order reduction over the ranges.
+  int i_lo, i_hi;
+  float* part;
+  int split_len;  // stations per range when a launch splits the set (grid z)
 };
 
 // ------------------------------------------------- folded interval sum
@@ -663,6 +670,20 @@ __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
       near_cur = D_next > r;
       D = D_next;
     };
+    if (a.i_lo > 0) {
+      // A station range that starts inside the set: the state of the
+      // interval (i_lo - 1, i_lo) and, for the explicit path, the values of
+      // station i_lo - 1, as the station before would have left them.
+      const float4 gp = __ldg(a.geo + a.i_lo - 1);
+      D = (T)gp.y;
+      fold_cur = folded_interval<T>(thr_fold, D, (T)gp.x);
+      near_cur = D > (T)gp.x;
+      if constexpr (kCarry) {
+#pragma unroll
+        for (int j = 0; j < CPT; ++j)
+          cell[j].template eval_y<WJ, WY, false>((T)gp.x, (T)gp.z, (T)gp.w, zpJ[j], zpY[j]);
+      }
+    }
     const int lane = threadIdx.x & 31;
     // Closes a chunk of stations: folds its partial sums into the totals.
     auto flush = [&]() {
@@ -686,9 +707,10 @@ __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
       const int tid = threadIdx.y * 32 + threadIdx.x;
       const StationCoef<float>* g0 = static_cast<const StationCoef<float>*>(a.gb[0]);
       const StationCoef<float>* g1 = static_cast<const StationCoef<float>*>(a.gb[MT::NIN > 1 ? 1 : 0]);
+      // chunks of S stations from i_lo (a multiple of S) to i_hi
       auto stage = [&](int ch, int buf) {
-        const int i0 = ch * S;
-        const int n = min(S, a.nr - i0);
+        const int i0 = a.i_lo + ch * S;
+        const int n = min(S, a.i_hi - i0);
         for (int t = tid; t < n * 32; t += kCellThreads) {
           const int st = t >> 5;
           const long long src = (long long)(i0 + st) * a.nf + min(fbase + (t & 31), a.nf - 1);
@@ -698,7 +720,7 @@ __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
         for (int t = tid; t < n; t += kCellThreads) cp_async16(&sb.geo[buf][t], a.geo + i0 + t);
         cp_async_commit();
       };
-      const int nch = (a.nr + S - 1) / S;
+      const int nch = (a.i_hi - a.i_lo + S - 1) / S;
       stage(0, 0);
       for (int ch = 0; ch < nch; ++ch) {
         const int buf = ch & 1;
@@ -708,8 +730,8 @@ __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
           cp_async_commit();  // one group per iteration keeps the count below
         cp_async_wait<1>();   // this thread's copies of chunk ch have landed
         __syncthreads();      // ... and everybody else's
-        const int i0 = ch * S;
-        const int n = min(S, a.nr - i0);
+        const int i0 = a.i_lo + ch * S;
+        const int n = min(S, a.i_hi - i0);
         if (c_valid) {
           // smallest r of the chunk (the input need not be sorted): at or
           // above s8w every station of the chunk has x >= 8 in every cell of
@@ -736,8 +758,8 @@ __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
         __syncthreads();  // buffer buf is refilled by the stage() of the next iteration
       }
     } else {
-      for (int i0 = 0; i0 < a.nr; i0 += kChunk) {
-        const int i1 = min(a.nr, i0 + kChunk);
+      for (int i0 = a.i_lo; i0 < a.i_hi; i0 += kChunk) {
+        const int i1 = min(a.i_hi, i0 + kChunk);
         float rmin = INFINITY;
         for (int t = i0 + lane; t < i1; t += 32) rmin = fminf(rmin, __ldg(a.rs + t));
         for (int o = 16; o > 0; o >>= 1) rmin = fminf(rmin, __shfl_xor_sync(0xffffffffu, rmin, o));
@@ -758,6 +780,15 @@ __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
       }
     }
     if (!c_valid) return;
+    if (a.part) {  // raw sums of this station range
+#pragma unroll
+      for (int j = 0; j < CPT; ++j)
+        if (f_valid && c0 + j < a.nc)
+#pragma unroll
+          for (int q = 0; q < MT::NACC; ++q)
+            a.part[((long long)q * a.nc + c0 + j) * a.nf + fi] = (float)tot[j][q];
+      return;
+    }
 #pragma unroll
     for (int j = 0; j < CPT; ++j) {
       const T gam = cell[j].gamma();
@@ -808,8 +839,8 @@ __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
       const float* g0 = static_cast<const float*>(a.gb[0]);
       const float* g1 = static_cast<const float*>(a.gb[MT::NIN > 1 ? 1 : 0]);
       auto stage = [&](int ch, int buf) {
-        const int i0 = ch * S;
-        const int n = min(S, a.nr - i0);
+        const int i0 = a.i_lo + ch * S;
+        const int n = min(S, a.i_hi - i0);
         for (int t = tid; t < n * 32; t += kCellThreads) {
           const int st = t >> 5;
           const long long src = (long long)(i0 + st) * a.nf + min(fbase + (t & 31), a.nf - 1);
@@ -819,7 +850,7 @@ __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
         for (int t = tid; t < n; t += kCellThreads) cp_async16(&sb.geo[buf][t], a.geo + i0 + t);
         cp_async_commit();
       };
-      const int nch = (a.nr + S - 1) / S;
+      const int nch = (a.i_hi - a.i_lo + S - 1) / S;
       stage(0, 0);
       for (int ch = 0; ch < nch; ++ch) {
         const int buf = ch & 1;
@@ -829,7 +860,7 @@ __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
           cp_async_commit();
         cp_async_wait<1>();
         __syncthreads();
-        const int n = min(S, a.nr - ch * S);
+        const int n = min(S, a.i_hi - a.i_lo - ch * S);
         if (c_valid) {
           float rmin = INFINITY;
           for (int t = lane; t < n; t += 32) rmin = fminf(rmin, sb.geo[buf][t].x);
@@ -850,8 +881,8 @@ __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
         __syncthreads();
       }
     } else {
-      for (int i0 = 0; i0 < a.nr; i0 += kChunk) {
-        const int i1 = min(a.nr, i0 + kChunk);
+      for (int i0 = a.i_lo; i0 < a.i_hi; i0 += kChunk) {
+        const int i1 = min(a.i_hi, i0 + kChunk);
         for (int i = i0; i < i1; ++i) {
           const long long gidx = (long long)i * a.nf + fi;
           const T q0 = __ldg(static_cast<const T*>(a.gb[0]) + gidx);
@@ -862,6 +893,15 @@ __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
       }
     }
     if (!c_valid) return;
+    if (a.part) {  // raw sums of this station range
+#pragma unroll
+      for (int j = 0; j < CPT; ++j)
+        if (f_valid && c0 + j < a.nc)
+#pragma unroll
+          for (int q = 0; q < MT::NACC; ++q)
+            a.part[((long long)q * a.nc + c0 + j) * a.nf + fi] = (float)tot[j][q];
+      return;
+    }
 #pragma unroll
     for (int j = 0; j < CPT; ++j) {
       const T gam = cell[j].gamma();

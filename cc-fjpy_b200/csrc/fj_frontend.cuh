@@ -25,8 +25,9 @@ int hilbert_rows_fft(const InDesc& in, int n, int es, int nr, int nf, int fstrid
                      float* dst, cudaStream_t s, Scratch& sc);
 
 // Device-resident transform (all pointers in args are device pointers);
-// cpt > 0 forces that variant of the FP32 kernel (velocities per thread).
-int fj_device(const ccfj_fj_args& a, cudaStream_t s, int cpt = 0);
+// cpt > 0 forces that variant of the FP32 kernel (velocities per thread),
+// nsplit > 0 that many station ranges (split launch, fixed-order sum).
+int fj_device(const ccfj_fj_args& a, cudaStream_t s, int cpt = 0, int nsplit = 0);
 // The argument checks of ccfj_fj_v1 (status and message as it returns them).
 int fj_validate(const ccfj_fj_args* a);
 

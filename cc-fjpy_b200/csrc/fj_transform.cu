@@ -61,10 +61,41 @@ __global__ void fj_prep_geom_kernel(const float* __restrict__ rs, int nr, float*
 
 template <int MODE, int ITYPE, typename T, int CPT>
 __global__ void __launch_bounds__(256, fj_min_blocks<T>()) fj_amortized_kernel(FjDev a) {
+  if (gridDim.z > 1) {
+    // split launch: CTA layer z sums stations [z L, (z + 1) L) into its own
+    // partial sums (fj_split_finish_kernel adds the layers in order)
+    a.i_lo = blockIdx.z * a.split_len;
+    a.i_hi = min(a.nr, a.i_lo + a.split_len);
+    a.part += (long long)blockIdx.z * ModeTraits<MODE>::NACC * a.nc * a.nf;
+  }
   // velocity tiles on grid x: the CTAs of one frequency tile run side by
   // side and share its station coefficients in L2
   fj_cells<MODE, ITYPE, T, CPT>(a, blockIdx.y * blockDim.x + threadIdx.x,
                                 (blockIdx.x * blockDim.y + threadIdx.y) * CPT);
+}
+
+// Sum of the station ranges of a split launch, in range order (the result
+// does not depend on how the ranges were scheduled), then the amplitude
+// gamma(k), the mode's combination and NaN at k = 0, as fj_cells finishes
+// an unsplit sum.
+template <int MODE>
+__global__ void fj_split_finish_kernel(const float* __restrict__ part, int nsplit,
+                                       const float* __restrict__ f, const float* __restrict__ c,
+                                       int nc, int nf, float* __restrict__ out) {
+  const int fi = blockIdx.x * 32 + threadIdx.x;
+  const int ci = blockIdx.y * 8 + threadIdx.y;
+  if (fi >= nf || ci >= nc) return;
+  constexpr int NACC = ModeTraits<MODE>::NACC;
+  const long long plane = (long long)nc * nf, at = (long long)ci * nf + fi;
+  float tot[2] = {0.f, 0.f};
+  for (int z = 0; z < nsplit; ++z)
+#pragma unroll
+    for (int q = 0; q < NACC; ++q) tot[q] += part[((long long)z * NACC + q) * plane + at];
+  Cell<float> cell;
+  cell.init(f[fi], c[ci]);
+  const float gam = cell.gamma();
+  float res[2] = {gam * tot[0], gam * tot[1]};
+  out[at] = cell.k == 0.0f ? __int_as_float(0x7fffffff) : finish<MODE, float>(res, 1.0f);
 }
 
 // ------------------------------------------ FP64 comparator (plain form)
@@ -190,7 +221,8 @@ std::atomic<int> g_force_cpt{0};
 template <int MODE, typename T, int CPT>
 void launch_amortized_cpt(int itype, const FjDev& d, cudaStream_t s) {
   const dim3 block(32, 8);
-  const dim3 grid(div_up(d.nc, 8 * CPT), div_up(d.nf, 32));
+  const int nsplit = d.part ? div_up(d.nr, d.split_len) : 1;
+  const dim3 grid(div_up(d.nc, 8 * CPT), div_up(d.nf, 32), nsplit);
   if (itype == 1)
     fj_amortized_kernel<MODE, 1, T, CPT><<<grid, block, 0, s>>>(d);
   else
@@ -233,12 +265,10 @@ int nin_of(int mode) { return (mode == CCFJ_MODE_J || mode == CCFJ_MODE_Y) ? 1 :
 }  // namespace
 
 // ------------------------------------------------------------ autotuner
-// The tuned table maps a problem class to the fastest velocities-per-thread
-// variant; classes are (mode, itype, log2 of nr, of nf, of nc).
+// The tuned table maps a problem class to the fastest tile choice --
+// velocities per thread and station ranges -- on a device; classes are
+// (mode, itype, log2 of nr, of nf, of nc).
 namespace {
-std::mutex g_tune_mu;
-std::map<long long, int> g_tune;
-
 long long tune_key(const ccfj_fj_args& a) {
   auto lg = [](long long v) {
     int b = 0;
@@ -258,15 +288,15 @@ int default_cpt_for(int mode, int itype) {
 }
 
 
+// A tuned choice is stored as cpt + 8 * nsplit (tuner "fj" of the table).
 int tuned_cpt(const ccfj_fj_args& a) {
-  std::lock_guard<std::mutex> lk(g_tune_mu);
-  auto it = g_tune.find(tune_key(a));
-  return it == g_tune.end() ? default_cpt_for(a.mode, a.itype) : it->second;
+  int choice = 0;
+  return tune_lookup("fj", tune_key(a), &choice) ? choice % 8 : default_cpt_for(a.mode, a.itype);
 }
 
-void record_tuned_cpt(const ccfj_fj_args& a, int cpt) {
-  std::lock_guard<std::mutex> lk(g_tune_mu);
-  g_tune[tune_key(a)] = cpt;
+int tuned_split(const ccfj_fj_args& a) {
+  int choice = 0;
+  return tune_lookup("fj", tune_key(a), &choice) ? choice / 8 : 0;
 }
 
 // The variant a transform runs: the caller's choice (the autotuner's
@@ -275,6 +305,39 @@ static int variant_for(const ccfj_fj_args& a, int cpt) {
   if (cpt > 0) return cpt;
   const int forced = g_force_cpt.load(std::memory_order_relaxed);
   return forced > 0 ? forced : tuned_cpt(a);
+}
+
+// Station ranges of one FP32 transform (split launches): split_choice if
+// given, else the tuned choice for the problem class, else enough ranges
+// that the grid fills the SMs' resident slots when the (velocity tile x
+// frequency tile) grid alone leaves them idle -- the largest n <= 4 with
+// n x CTAs <= 1.1 x slots and ranges of at least two station chunks.
+constexpr int kSplitAlign = 32;  // multiple of every staged chunk (16 or 32 stations)
+static int sm_count() {
+  static std::atomic<int> cached{0};
+  int v = cached.load(std::memory_order_relaxed);
+  if (v == 0) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0)
+      v = 148;
+    cached.store(v, std::memory_order_relaxed);
+  }
+  return v;
+}
+std::atomic<int> g_force_split{0};
+static int split_for(const ccfj_fj_args& a, int cpt, int split_choice) {
+  if (split_choice > 0) return split_choice;
+  const int forced = g_force_split.load(std::memory_order_relaxed);
+  if (forced > 0) return forced;
+  const int tuned = tuned_split(a);
+  if (tuned > 0) return tuned;
+  const long long ctas = (long long)div_up(a.nc, 8 * cpt) * div_up(a.nf, 32);
+  const long long slots = (long long)sm_count() * CCFJ_FJ_MIN_BLOCKS;
+  int n = 1;
+  for (int k = 2; k <= 4; ++k)
+    if (k * ctas * 10 <= slots * 11 && a.nr >= 2 * kSplitAlign * k) n = k;
+  return n;
 }
 
 // Bytes of the itype-1 per-station geometry and per-frequency fold
@@ -339,7 +402,7 @@ int prep_interval_data(const ccfj_fj_args& a, FjDev& d, const InDesc* in, int ni
 
 // Device-resident transform: every pointer in `a` is a device pointer.
 // cpt > 0 runs that variant (velocities per thread) of the FP32 kernel.
-int fj_device(const ccfj_fj_args& a, cudaStream_t s, int cpt_choice) {
+int fj_device(const ccfj_fj_args& a, cudaStream_t s, int cpt_choice, int split_choice) {
   const int nin = nin_of(a.mode);
   Scratch sc(s);
   float* drs = sc.get_n<float>(a.nr + 1);
@@ -362,6 +425,10 @@ int fj_device(const ccfj_fj_args& a, cudaStream_t s, int cpt_choice) {
   d.nf = a.nf;
   d.nc = a.nc;
   d.tau = a.tau > 0 ? a.tau : (a.precision == CCFJ_PREC_FP32 ? kDefaultTau32 : kDefaultTau64);
+  d.i_lo = 0;
+  d.i_hi = a.nr;
+  d.part = nullptr;
+  d.split_len = a.nr;
 
   InDesc in[2];
   const long long col0 = (long long)a.col_begin * a.fstride * a.u_es;  // first computed column
@@ -403,6 +470,17 @@ int fj_device(const ccfj_fj_args& a, cudaStream_t s, int cpt_choice) {
   }
 
   const int cpt = variant_for(a, cpt_choice);
+  if (a.precision == CCFJ_PREC_FP32) {
+    const int nsplit = split_for(a, cpt, split_choice);
+    if (nsplit > 1) {
+      d.split_len = (int)div_up(div_up(a.nr, nsplit), kSplitAlign) * kSplitAlign;
+      const int n = (int)div_up(a.nr, d.split_len);
+      if (n > 1) {
+        d.part = sc.get_n<float>((size_t)n * nin_of(a.mode) * a.nc * a.nf);
+        if (!d.part) return CCFJ_ERR_ALLOC;
+      }
+    }
+  }
   prof_begin(s);
   switch (a.mode) {
     case CCFJ_MODE_J:
@@ -424,6 +502,32 @@ int fj_device(const ccfj_fj_args& a, cudaStream_t s, int cpt_choice) {
   prof_end(s);
   count_launch();
   CCFJ_LAUNCH_CHECK("fj transform kernel");
+  if (d.part) {
+    const int n = (int)div_up(a.nr, d.split_len);
+    const dim3 fg(div_up(a.nf, 32), div_up(a.nc, 8)), fb(32, 8);
+    switch (a.mode) {
+      case CCFJ_MODE_J:
+        fj_split_finish_kernel<CCFJ_MODE_J><<<fg, fb, 0, s>>>(d.part, n, a.f, a.c, a.nc, a.nf, a.out);
+        break;
+      case CCFJ_MODE_Y:
+        fj_split_finish_kernel<CCFJ_MODE_Y><<<fg, fb, 0, s>>>(d.part, n, a.f, a.c, a.nc, a.nf, a.out);
+        break;
+      case CCFJ_MODE_J_MINUS_Y:
+        fj_split_finish_kernel<CCFJ_MODE_J_MINUS_Y><<<fg, fb, 0, s>>>(d.part, n, a.f, a.c, a.nc,
+                                                                     a.nf, a.out);
+        break;
+      case CCFJ_MODE_ABS_J:
+        fj_split_finish_kernel<CCFJ_MODE_ABS_J><<<fg, fb, 0, s>>>(d.part, n, a.f, a.c, a.nc, a.nf,
+                                                                 a.out);
+        break;
+      default:
+        fj_split_finish_kernel<CCFJ_MODE_ABS_H><<<fg, fb, 0, s>>>(d.part, n, a.f, a.c, a.nc, a.nf,
+                                                                 a.out);
+        break;
+    }
+    count_launch();
+    CCFJ_LAUNCH_CHECK("fj_split_finish_kernel");
+  }
 
   if (a.normalize) {
     fj_normalize_kernel<<<div_up(a.nf, 32), dim3(32, 8), 0, s>>>(a.out, a.nc, a.nf);
@@ -840,8 +944,13 @@ CCFJ_API int ccfj_autotune_fj_v1(const ccfj_fj_args* args, void* stream, int* be
   if (!args->device_ptrs)
     return ccfj::set_error(CCFJ_ERR_INVALID, "ccfj_autotune_fj_v1: needs device pointers");
   cudaStream_t s = (cudaStream_t)stream;
-  const int cands[3] = {1, 2, 4};
-  int best = 2;
+  // candidates: 1, 2 or 4 velocities per thread, times 1 to 8 station
+  // ranges where the unsplit grid leaves resident slots idle
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess)
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long slots = (long long)sms * CCFJ_FJ_MIN_BLOCKS;
+  int best = 2, best_split = 1;
   float best_t = 1e30f;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
@@ -849,29 +958,54 @@ CCFJ_API int ccfj_autotune_fj_v1(const ccfj_fj_args* args, void* stream, int* be
     return ccfj::set_error(CCFJ_ERR_CUDA, "ccfj_autotune_fj_v1: cudaEventCreate failed: %s",
                            cudaGetErrorString(cudaGetLastError()));
   }
+  const int cands[3] = {1, 2, 4};
+  const int splits[6] = {1, 2, 3, 4, 6, 8};
   for (int c : cands) {
-    float t = 1e30f;
-    for (int rep = 0; rep < 3 && st == CCFJ_OK; ++rep) {
-      cudaEventRecord(e0, s);
-      st = ccfj::fj_device(*args, s, c);
-      cudaEventRecord(e1, s);
-      if (cudaEventSynchronize(e1) != cudaSuccess) st = CCFJ_ERR_CUDA;
-      float ms = 0;
-      cudaEventElapsedTime(&ms, e0, e1);
-      if (rep > 0) t = std::min(t, ms);  // the first run is a warm-up
+    const long long ctas = (long long)ccfj::div_up(args->nc, 8 * c) * ccfj::div_up(args->nf, 32);
+    for (int n : splits) {
+      if (n > 1 && (n * ctas > 2 * slots || args->nr < 2 * 32 * n)) continue;
+      float t = 1e30f;
+      for (int rep = 0; rep < 3 && st == CCFJ_OK; ++rep) {
+        cudaEventRecord(e0, s);
+        st = ccfj::fj_device(*args, s, c, n);
+        cudaEventRecord(e1, s);
+        if (cudaEventSynchronize(e1) != cudaSuccess) st = CCFJ_ERR_CUDA;
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (rep > 0) t = std::min(t, ms);  // the first run is a warm-up
+      }
+      if (st != CCFJ_OK) break;
+      if (t < best_t) {
+        best_t = t;
+        best = c;
+        best_split = n;
+      }
     }
     if (st != CCFJ_OK) break;
-    if (t < best_t) {
-      best_t = t;
-      best = c;
-    }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   if (st != CCFJ_OK) return st;
-  ccfj::record_tuned_cpt(*args, best);
+  st = ccfj::tune_record("fj", ccfj::tune_key(*args), best + 8 * best_split, best_t);
   if (best_cpt) *best_cpt = best;
   if (best_ms) *best_ms = best_t;
+  return st;
+}
+
+CCFJ_API int ccfj_set_fj_split(int nsplit) {
+  if (nsplit < 0 || nsplit > 64)
+    return ccfj::set_error(CCFJ_ERR_INVALID, "ccfj_set_fj_split: nsplit must be 0..64");
+  ccfj::g_force_split.store(nsplit, std::memory_order_relaxed);
+  return CCFJ_OK;
+}
+
+CCFJ_API int ccfj_tuned_choice_fj(const ccfj_fj_args* args, int* cpt, int* nsplit) {
+  ccfj::clear_error();
+  int st = ccfj::validate(args);
+  if (st != CCFJ_OK) return st;
+  const int c = ccfj::variant_for(*args, 0);
+  if (cpt) *cpt = c;
+  if (nsplit) *nsplit = args->precision == CCFJ_PREC_FP32 ? ccfj::split_for(*args, c, 0) : 1;
   return CCFJ_OK;
 }
 
@@ -984,6 +1118,10 @@ static int fj_noalloc(const ccfj_fj_args& a, cudaStream_t s) {
   d.nf = a.nf;
   d.nc = a.nc;
   d.tau = a.tau > 0 ? a.tau : kDefaultTau32;
+  d.i_lo = 0;
+  d.i_hi = a.nr;
+  d.part = nullptr;
+  d.split_len = a.nr;
   InDesc in[2];
   void* gbuf[2] = {nullptr, nullptr};
   for (int j = 0; j < nin; ++j) {

@@ -155,8 +155,10 @@ CCFJ_API int ccfj_fj_batch_v1(const ccfj_batch_args *args, void *stream);
 CCFJ_API int ccfj_batch_graph_cache_clear(void);
 /* Runs the batch (device pointers; out is overwritten) with 1, 2 and 4
  * velocities per thread, records the fastest for the batch's class (mode,
- * itype and the powers of two of total pairs, nsets, nf and nc) for later
- * calls of this process that pass variant 0, and returns it and its time. */
+ * itype and the powers of two of total pairs, nsets, nf and nc) on this
+ * device for later calls that pass variant 0 -- in this process, and in
+ * later ones through the persistent table of ccfj_set_tune_cache -- and
+ * returns it and its time. */
 CCFJ_API int ccfj_autotune_batch_v1(const ccfj_batch_args *args, void *stream,
                                     int *best_variant, float *best_ms);
 
@@ -335,16 +337,35 @@ CCFJ_API int CrossCorrelation(ccfj_cc_data data);
 CCFJ_API int ccfj_cc_fj_noise_v1(const ccfj_cc_args *cc, const ccfj_fj_args *fj, void *stream);
 
 /* ------------------------------------------------------------- tuning
- * The FP32 kernels come in variants that give each thread 1, 2 or 4
- * velocities. ccfj_autotune_fj_v1 runs every variant on the given problem
- * (device pointers; out is overwritten), records the fastest for the
- * problem's class (mode, itype and the powers of two of nr, nf, nc) for all
- * later calls of this process, and returns it. ccfj_set_fj_variant(cpt)
- * forces a variant (0 restores the tuned choice, or the default: 2 for
- * itype 1, 4 for itype 0). */
+ * Tile choices of the FP32 transform: 1, 2 or 4 velocities per thread, and
+ * the number of station ranges (split launch: ranges of whole 32-station
+ * chunks summed in a fixed order by a second kernel, so a given choice
+ * gives the same result on every run). ccfj_autotune_fj_v1 times every
+ * velocities-per-thread variant with 1 range and, where the unsplit grid
+ * leaves resident slots idle, with 2-8 ranges, on the given problem (device
+ * pointers; out is overwritten), records the fastest for the problem's
+ * class (mode, itype and the powers of two of nr, nf, nc) on this device,
+ * and returns its velocities per thread and time. Untuned classes use 2
+ * (itype 1) or 4 (itype 0) velocities per thread and as many ranges (at
+ * most 4) as fill the SMs' resident slots without starting another wave.
+ * ccfj_set_fj_variant(cpt) forces a velocities-per-thread variant (0
+ * restores the tuned or default choice).
+ *
+ * Persistence: ccfj_set_tune_cache(path) names a text table that both
+ * autotuners write every result to and that later calls (in this or any
+ * later process) read per device, one line per (device name, tuner,
+ * problem class); NULL returns to the default, the file named by the
+ * environment variable CCFJ_TUNE_CACHE, or none. ccfj_tuned_choice_fj
+ * reports the choice a call with these arguments would run. No
+ * counterparts in the reference, which has no tuning. */
 CCFJ_API int ccfj_autotune_fj_v1(const ccfj_fj_args *args, void *stream, int *best_cpt,
                                  float *best_ms);
 CCFJ_API int ccfj_set_fj_variant(int cpt);
+/* Forces the number of station ranges of FP32 transforms (1 = unsplit;
+ * 0 restores the tuned or default choice). */
+CCFJ_API int ccfj_set_fj_split(int nsplit);
+CCFJ_API int ccfj_set_tune_cache(const char *path);
+CCFJ_API int ccfj_tuned_choice_fj(const ccfj_fj_args *args, int *cpt, int *nsplit);
 
 /* ------------------------------------------------------------------ misc */
 CCFJ_API const char *ccfj_last_error(void);

@@ -10,6 +10,7 @@
   the host-memory call bit for bit.
 """
 import ctypes
+import os
 import warnings
 
 import numpy as np
@@ -19,6 +20,7 @@ import cases
 
 pytestmark = pytest.mark.gpu
 VAR_TOL = 2e-5
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def _err(y, ref):
@@ -176,3 +178,82 @@ def test_single_set_autotuner(lib):
     _lib.check(lib.ccfj_autotune_fj_v1(ctypes.byref(a), None, ctypes.byref(best),
                                        ctypes.byref(ms)))
     assert best.value in (1, 2, 4) and ms.value > 0
+
+
+def _mid_case():
+    """300 pairs (1-50 km) x 64 f x 70 c: few CTAs, enough stations for
+    8 ranges of 32."""
+    rng = np.random.default_rng(21)
+    r = rng.uniform(1e3, 5e4, 300)
+    f = np.linspace(0.02, 1.0, 64)
+    c = np.linspace(1000.0, 5000.0, 70)
+    return cases.noise_spectra(rng, r, f, sigma=0.1), r, c, f
+
+
+@pytest.mark.parametrize("itype,func", [(1, 0), (1, 1), (0, 0)])
+@pytest.mark.parametrize("nsplit", [2, 3, 8])
+def test_split_launch_matches_unsplit_and_oracle(lib, itype, func, nsplit):
+    """Station ranges summed in a fixed order: the same spectrum as the
+    unsplit launch (to rounding), within 1e-4 of the FP64 oracle, and the
+    same bits on a second run."""
+    import ccfj
+    import fj_oracle as O
+    uf, r, c, f = _mid_case()
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        try:
+            assert lib.ccfj_set_fj_split(1) == 0
+            base = ccfj.fj_noise(uf, r, c, f, itype=itype, func=func)
+            assert lib.ccfj_set_fj_split(nsplit) == 0
+            y = ccfj.fj_noise(uf, r, c, f, itype=itype, func=func)
+            y2 = ccfj.fj_noise(uf, r, c, f, itype=itype, func=func)
+        finally:
+            lib.ccfj_set_fj_split(0)
+        y64 = O.fj_noise(uf, r, c, f, itype=itype, func=func)
+    assert _err(y, base) <= 1e-5
+    assert O.rel_error(y, y64) <= 1e-4
+    assert np.array_equal(y, y2)
+
+
+def test_tuned_choice_is_reused_by_another_process(tmp_path):
+    """The autotuner writes its choice to the table named by
+    CCFJ_TUNE_CACHE; a second process reads it back for the same class."""
+    import subprocess
+    import sys
+    cache = tmp_path / "tune.txt"
+    prog = r'''
+import ctypes, sys, numpy as np, torch
+sys.path[:0] = [%r, %r]
+import cases
+from ccfj import _lib
+lib = _lib.load()
+rng = np.random.default_rng(21)
+r = np.sort(rng.uniform(1e3, 5e4, 300)); f = np.linspace(0.02, 1.0, 64)
+c = np.linspace(1000.0, 5000.0, 70); uf = cases.noise_spectra(rng, r, f, sigma=0.1)
+T = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in dict(
+    u=uf.view(np.float32), r=r.astype(np.float32), f=f.astype(np.float32),
+    c=c.astype(np.float32)).items()}
+out = torch.empty((70, 64), device="cuda")
+a = _lib.FjArgs(); a.struct_size = ctypes.sizeof(a)
+a.nr, a.nf, a.nc, a.itype, a.mode, a.precision, a.normalize, a.device_ptrs = 300, 64, 70, 1, 0, 0, 1, 1
+a.u[0] = T["u"].data_ptr(); a.u_ld, a.u_rows, a.u_es, a.u_ncols, a.fstride = 128, 300, 2, 64, 1
+a.r, a.f, a.c, a.out = T["r"].data_ptr(), T["f"].data_ptr(), T["c"].data_ptr(), out.data_ptr()
+cpt, ns = ctypes.c_int(), ctypes.c_int()
+if sys.argv[1] == "tune":
+    ms = ctypes.c_float()
+    _lib.check(lib.ccfj_autotune_fj_v1(ctypes.byref(a), None, ctypes.byref(cpt), ctypes.byref(ms)))
+_lib.check(lib.ccfj_tuned_choice_fj(ctypes.byref(a), ctypes.byref(cpt), ctypes.byref(ns)))
+print(cpt.value, ns.value)
+''' % (os.path.join(REPO, "cc-fjpy_b200"), os.path.join(REPO, "tests"))
+    env = dict(os.environ, CCFJ_TUNE_CACHE=str(cache))
+    first = subprocess.run([sys.executable, "-c", prog, "tune"], env=env, capture_output=True,
+                           text=True, timeout=600)
+    assert first.returncode == 0, first.stderr
+    second = subprocess.run([sys.executable, "-c", prog, "query"], env=env, capture_output=True,
+                            text=True, timeout=600)
+    assert second.returncode == 0, second.stderr
+    assert first.stdout.split() == second.stdout.split()
+    line = [ln for ln in cache.read_text().splitlines() if ln.startswith("ccfj-tune-v1 ")]
+    assert len(line) == 1 and " fj " in line[0]
+    cpt, ns = (int(v) for v in second.stdout.split())
+    assert int(line[0].split()[4]) == cpt + 8 * ns
