@@ -151,6 +151,8 @@ __global__ void __launch_bounds__(256, fj_min_blocks<float>()) fj_batch_persiste
     const long long o = bd.off[b];
     FjDev a = bd.base;
     a.nr = (int)(bd.off[b + 1] - o);
+    a.i_lo = 0;  // the whole set
+    a.i_hi = a.nr;
     a.rs += o;
     a.drs += o;
     a.geo += o;

@@ -572,6 +572,54 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
+// The x >= 8 station step of the J-basis modes for CPT cells, two cells per
+// paired FP32 instruction (fjs::eval_large_scaled_pair_j): the station
+// values y0, y1 of every cell (into Jzs) and the folded-sum accumulation of
+// each input -- acc0 += (A - k^2 C) y0, acc1 += B y1 -- exactly as the
+// scalar loop computes them. The primary template (FP64 cells, odd CPT) is
+// never called.
+template <bool PAIRED>
+struct PairedStationJ {
+  template <int NIN, int CPT, typename CellT, typename Q, typename AccT, typename ZT>
+  __device__ __forceinline__ static void run(const CellT*, float, float, const Q&, const Q&, AccT&,
+                                             AccT&, ZT&) {}
+};
+#if defined(FJS_HAVE_PAIRED)
+template <>
+struct PairedStationJ<true> {
+  template <int NIN, int CPT>
+  __device__ __forceinline__ static void run(const Cell<float>* cell, float r, float rinv,
+                                             const StationCoef<float>& q0,
+                                             const StationCoef<float>& q1, float (&acc0)[CPT][2],
+                                             float (&acc1)[CPT][2], ZB<float> (&Jzs)[CPT]) {
+#pragma unroll
+    for (int j = 0; j < CPT; j += 2) {
+      const fjs::PairPhase ph{make_float2(cell[j].q_hi, cell[j + 1].q_hi),
+                              make_float2(-cell[j].q_hi, -cell[j + 1].q_hi),
+                              make_float2(cell[j].q_lo, cell[j + 1].q_lo),
+                              make_float2(cell[j].s8, cell[j + 1].s8)};
+      fjs::ZB2 J2;
+      fjs::eval_large_scaled_pair_j(ph, r, rinv, J2);
+      Jzs[j] = ZB<float>{J2.z0.x, J2.z1.x, 0.0f};
+      Jzs[j + 1] = ZB<float>{J2.z0.y, J2.z1.y, 0.0f};
+      const float2 nk2 = make_float2(-cell[j].k2, -cell[j + 1].k2);
+#pragma unroll
+      for (int q = 0; q < NIN; ++q) {  // ABS_J: the second input shares the station values
+        const StationCoef<float>& sc = q == 0 ? q0 : q1;
+        const float2 u = fjs::pfma(nk2, fjs::psplat(sc.C), fjs::psplat(sc.A));
+        const float2 a0 = fjs::pfma(u, J2.z0, make_float2(acc0[j][q], acc0[j + 1][q]));
+        const float2 a1 =
+            fjs::pfma(fjs::psplat(sc.B), J2.z1, make_float2(acc1[j][q], acc1[j + 1][q]));
+        acc0[j][q] = a0.x;
+        acc0[j + 1][q] = a0.y;
+        acc1[j][q] = a1.x;
+        acc1[j + 1][q] = a1.y;
+      }
+    }
+  }
+};
+#endif
+
 // CPT cells (f, c), (f, c + 1), ... per thread share the per-station loads.
 // The transform of the CPT cells (fi, c0), (fi, c0 + 1), ... of one data
 // set; shared by the grid kernel below and the persistent batch kernel.
@@ -610,6 +658,14 @@ __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
       s8w = fmax(s8w, cell[j].s8);
     }
     for (int o = 16; o > 0; o >>= 1) s8w = fmax(s8w, __shfl_xor_sync(0xffffffffu, s8w, o));
+    // Paired FP32 arithmetic (two cells per FFMA2 / FMUL2 / FADD2) for the
+    // J-basis modes with an even number of cells per thread; the Y basis
+    // and the explicit path stay scalar. Bitwise the scalar result.
+#ifndef CCFJ_PAIRED
+#define CCFJ_PAIRED 1
+#endif
+    constexpr bool kPaired = CCFJ_PAIRED && sizeof(T) == 4 && CPT % 2 == 0 && WJ && !WY &&
+                             (MODE == CCFJ_MODE_J || MODE == CCFJ_MODE_ABS_J);
     // The explicit path needs station i-1's values: single-basis modes carry
     // them (2 registers per cell); two-basis modes, short of registers,
     // evaluate station i-1 again when an explicit interval comes.
@@ -628,14 +684,30 @@ __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
       const T r = gm.x, D_next = gm.y;
       const long long qi = (long long)i * a.nf;
       const T dl8 = fabs(D) * d8;
+      ZB<T> Jzs[CPT], Yzs[CPT];
+#if defined(FJS_HAVE_PAIRED)
+      if constexpr (kPaired && LARGE) {
+        // two cells per paired instruction (x >= 8 in every cell of the warp)
+        PairedStationJ<kPaired>::template run<MT::NIN, CPT>(cell, (float)r, (float)gm.z, q0, q1,
+                                                             acc0, acc1, Jzs);
+      } else
+#endif
+      {
+#pragma unroll
+        for (int j = 0; j < CPT; ++j) {
+          ZB<T> Jz{}, Yz{};
+          cell[j].template eval_y<WJ, WY, LARGE>(r, (T)gm.z, (T)gm.w, Jz, Yz);
+          const T u0 = fjs::fmaT(-cell[j].k2, q0.C, q0.A);
+          const T u1 = MT::NIN > 1 ? fjs::fmaT(-cell[j].k2, q1.C, q1.A) : T(0);
+          accumulate_station<MODE, T>(acc0[j], u0, u1, WJ ? Jz.z0 : T(0), WY ? Yz.z0 : T(0));
+          accumulate_station<MODE, T>(acc1[j], q0.B, q1.B, WJ ? Jz.z1 : T(0), WY ? Yz.z1 : T(0));
+          Jzs[j] = Jz;
+          Yzs[j] = Yz;
+        }
+      }
 #pragma unroll
       for (int j = 0; j < CPT; ++j) {
-        ZB<T> Jz{}, Yz{};
-        cell[j].template eval_y<WJ, WY, LARGE>(r, (T)gm.z, (T)gm.w, Jz, Yz);
-        const T u0 = fjs::fmaT(-cell[j].k2, q0.C, q0.A);
-        const T u1 = MT::NIN > 1 ? fjs::fmaT(-cell[j].k2, q1.C, q1.A) : T(0);
-        accumulate_station<MODE, T>(acc0[j], u0, u1, WJ ? Jz.z0 : T(0), WY ? Yz.z0 : T(0));
-        accumulate_station<MODE, T>(acc1[j], q0.B, q1.B, WJ ? Jz.z1 : T(0), WY ? Yz.z1 : T(0));
+        ZB<T> Jz = Jzs[j], Yz = Yzs[j];
         const bool clJ = dl8 >= cell[j].s8;
         const bool clY = clJ || near_cur;  // Y0 is singular at 0
         const bool exJ = WJ && (clJ || !fold_cur), exY = WY && (clY || !fold_cur);

@@ -434,4 +434,80 @@ FJ_HD void eval_station_f64(double x, double t, ZB<double>& J, ZB<double>& Y) {
   }
 }
 
+// ------------------------------------------ paired evaluation (sm_100)
+// Two cells (two velocities of one frequency) at one station: every FP32
+// operation of eval_large_scaled_f32 on both lanes as one paired
+// instruction (FFMA2 / FMUL2 / FADD2 on sm_100). Each lane performs exactly
+// the scalar function's operations in the same order with the same
+// rounding -- negated quantities come from negated inputs or coefficients,
+// which round-to-nearest maps to exactly negated results -- so the pair
+// equals two scalar calls bit for bit, with about half the instructions.
+#if defined(__CUDACC__)
+#if !defined(__CUDA_ARCH__) || __CUDA_ARCH__ >= 1000
+#define FJS_HAVE_PAIRED 1
+__device__ __forceinline__ float2 pfma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 pmul(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 padd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 psplat(float v) { return make_float2(v, v); }
+
+template <int N>
+__device__ __forceinline__ float2 phorner(const float (&c)[N], float2 v) {
+  float2 acc = psplat(c[N - 1]);
+#pragma unroll
+  for (int i = N - 2; i >= 0; --i) acc = pfma(acc, v, psplat(c[i]));
+  return acc;
+}
+// The same with every coefficient negated: exactly -phorner(c, v).
+template <int N>
+__device__ __forceinline__ float2 phorner_neg(const float (&c)[N], float2 v) {
+  float2 acc = psplat(-c[N - 1]);
+#pragma unroll
+  for (int i = N - 2; i >= 0; --i) acc = pfma(acc, v, psplat(-c[i]));
+  return acc;
+}
+
+struct ZB2 {
+  float2 z0, z1;
+};
+
+// Per-pair constants: the phase factor q = f / c as a double-float
+// (q_hi, q_lo), -q_hi, and s8 = 8 / k of each lane's cell.
+struct PairPhase {
+  float2 qhi, nqhi, qlo, s8;
+};
+
+// eval_large_scaled_f32<true, false, true> (need_b false) of both lanes at
+// the station r (1/r = rinv): y0 = J0 / M and y1 = J1 / M, x >= 8 in both.
+__device__ __forceinline__ void eval_large_scaled_pair_j(const PairPhase& ph, float r, float rinv,
+                                                         ZB2& J) {
+  const float2 rr = psplat(r);
+  // p_hi + p_lo = q r (the scalar: p_hi = q_hi r, e = fma(q_hi, r, -p_hi),
+  // p_lo = fma(q_lo, r, e))
+  const float2 p_hi = pmul(ph.qhi, rr);
+  const float2 np_hi = pmul(ph.nqhi, rr);  // -p_hi exactly
+  const float2 p_lo = pfma(ph.qlo, rr, pfma(ph.qhi, rr, np_hi));
+  // chi_cycles_f32: (p_hi - n) + (p_lo - 1/8), n = (p_hi + 1.5 2^23) - 1.5 2^23;
+  // -n = (-p_hi - 1.5 2^23) + 1.5 2^23 exactly
+  const float kMagic = 12582912.0f;
+  const float2 nn = padd(padd(np_hi, psplat(-kMagic)), psplat(kMagic));
+  const float2 u = padd(padd(p_hi, nn), padd(p_lo, psplat(-0.125f)));
+  float2 sn, cs;
+  sincos_cycles_f32(u.x, sn.x, cs.x);
+  sincos_cycles_f32(u.y, sn.y, cs.y);
+  const float2 sv = pmul(ph.s8, psplat(rinv));  // s = 8 / x
+  const float2 z = pmul(sv, sv);
+  constexpr float cp0[] = FJC_F32_L_P0;
+  constexpr float cq0[] = FJC_F32_L_Q0;
+  constexpr float cp1[] = FJC_F32_L_P1;
+  constexpr float cq1[] = FJC_F32_L_Q1;
+  const float2 P0 = phorner(cp0, z);
+  const float2 nQ0 = pmul(phorner_neg(cq0, z), sv);  // -Q0
+  const float2 P1 = phorner(cp1, z);
+  const float2 Q1 = pmul(phorner(cq1, z), sv);
+  J.z0 = pfma(P0, cs, pmul(nQ0, sn));  // fma(P0, cs, -Q0 sn)
+  J.z1 = pfma(P1, sn, pmul(Q1, cs));   // fma(P1, sn, Q1 cs)
+}
+#endif
+#endif
+
 }  // namespace fjs
