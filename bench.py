@@ -659,17 +659,17 @@ def measure_mwfj(lib, torch, dev, sp, peak, bf16, args):
     te, ye = _time_host_calls(lambda: _quiet(ccfj.MWFJ, u, r, c, f, wl["Fs"], nwin, wl["winl"],
                                              wl["winr"], wl["taper"]), 3, 1)
     # tensor work: per frequency a (nc x K) (K x 2 nwin) product, K = 2 (ntr - 1),
-    # in three bf16 passes (hi.hi + hi.lo + lo.hi)
+    # in three fp16 passes (hi.hi + hi.lo + lo.hi)
     gemm = 2.0 * nc * (2 * nwin) * (2 * (ntr - 1)) * nf
     tc_ach = 3 * gemm / ks / 1e12
     gen = FLOPS_E1 * float(ntr) * nf * nc
     rl = _fp32_roofline(gen, ks, peak, "fj_mw_tc_kernel (A-operand generation on the FP32 pipe, "
-                        "tcgen05 BF16x3 contraction)", FLOPS_E1)
+                        "tcgen05 FP16x3 contraction)", FLOPS_E1)
     rl["flops_note"] = ("FP32 figure: the station evaluations E = 104 flops per (f, c, pair), "
                         "shared by all windows")
     rl["tensor"] = {"achieved": tc_ach, "peak": bf16[0], "unit": "TFLOP/s", "frac": tc_ach / bf16[0],
                     "peak_source": bf16[1], "flops": 3 * gemm,
-                    "note": "2 nc (2 nwin) 2 (ntr - 1) nf algorithmic flops, x3 for BF16x3"}
+                    "note": "2 nc (2 nwin) 2 (ntr - 1) nf algorithmic flops, x3 for the hi/lo split (FP16x3); the dense fp16 and bf16 peaks are equal"}
     run.res = {
         "workload": "MWFJ itype=1 func=0: 1000 traces x 16384 samples at 10 Hz (r 5-1500 km), "
                     "64 windows per trace (200-2000 samples, taper 0.9), bins 0-1023, nc=2000 "
@@ -1140,6 +1140,65 @@ def run_ours(args, rank, world):
     return 0
 
 
+def run_profile_extra(args):
+    """Reduced cases for ncu captures of the kernels the main workloads do
+    not launch: 'noise0' = the trapezoid (itype 0) transform of the first 512
+    frequencies of the large-array workload; 'eq_short' = fj_earthquake on
+    500 traces of 512 samples (radix-2 FFT) and of 3000 samples (direct
+    DFT), 200 bins, 400 velocities; 'small' = the small-array workload
+    (split launch over station ranges); 'cc_direct' = cross-correlation of
+    50 stations x 86,400 samples in windows of 3001 samples (direct
+    transform of the requested bins)."""
+    import torch
+    import ccfj
+    from ccfj import _lib
+    lib = _lib.load()
+    sp = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    n = args.warmup + args.steps
+    if args.profile_case == "noise0":
+        uf, r, f, c = workload()
+        nf = 512
+        idx = np.argsort(r)
+        T = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in dict(
+            u=uf.view(np.float32), perm=idx.astype(np.int64), r=r[idx].astype(np.float32),
+            f=f.astype(np.float32), c=c.astype(np.float32)).items()}
+        out = torch.empty((NC, nf), device="cuda")
+        a = _fj_args(NPAIRS, nf, NC, 0, _lib.MODE_J, T["u"].data_ptr(), 2 * NF, 2,
+                     T["perm"].data_ptr(), T["r"], T["f"], T["c"], out)
+        for _ in range(n):
+            _lib.check(lib.ccfj_fj_v1(ctypes.byref(a), sp))
+    elif args.profile_case == "small":
+        uf, r, f, c = workload_small()
+        T = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in dict(
+            u=uf.view(np.float32), r=r.astype(np.float32), f=f.astype(np.float32),
+            c=c.astype(np.float32)).items()}
+        out = torch.empty((len(c), len(f)), device="cuda")
+        a = _fj_args(len(r), len(f), len(c), 1, _lib.MODE_J, T["u"].data_ptr(), 2 * len(f), 2,
+                     None, T["r"], T["f"], T["c"], out)
+        for _ in range(n):
+            _lib.check(lib.ccfj_fj_v1(ctypes.byref(a), sp))
+    elif args.profile_case == "eq_short":
+        import cases
+        rng = np.random.default_rng(13)
+        for npts in (512, 3000):
+            r = np.exp(rng.uniform(np.log(1e4), np.log(5e5), 500))
+            u = cases.ricker_records(rng, r, npts, 20.0)
+            f = 20.0 * np.arange(200) / npts
+            c = np.linspace(2000.0, 5000.0, 400)
+            for _ in range(n):
+                _quiet(ccfj.fj_earthquake, u, r, c, f)
+    else:  # cc_direct
+        nsta, npts, fftlen = 50, 86400, 3001
+        data = np.random.default_rng(17).standard_normal(nsta * npts, dtype=np.float32)
+        se = np.tile([0, npts], nsta).astype(np.int32)
+        pairs = ccfj.GetStationPairs(nsta)
+        for _ in range(n):
+            ccfj.CC(npts, nsta, 500, fftlen, pairs, se, data.copy(), overlaprate=0.5)
+    torch.cuda.synchronize()
+    print("profile case %s done: %d calls" % (args.profile_case, n))
+    return 0
+
+
 def run_profile_case(args):
     """The device transform on the first 512 frequencies of the workload
     (19,900 pairs, 1000 velocities; 163 MB of spectra, 163 MB of station
@@ -1296,14 +1355,16 @@ def main():
     ap.add_argument("--headline-only", action="store_true",
                     help="report the headline workload without the `configs` object")
     ap.add_argument("--profile-case", nargs="?", const="noise", default=None,
-                    choices=("noise", "hilbert", "mwfj", "mwfj_cc", "batch", "cc"),
+                    choices=("noise", "hilbert", "mwfj", "mwfj_cc", "batch", "cc", "noise0",
+                             "eq_short", "small", "cc_direct"),
                     help="run a reduced case for ncu captures: 'noise' = the device transform "
                          "on the first 512 frequencies of the workload (steps launches, no "
                          "extras); 'mwfj' = the MWFJ configuration with 8 windows and 256 bins; "
                          "'hilbert' = the same with func 1 (device Hilbert transform); 'mwfj_cc' "
                          "= the MWFJ case with func 1 (CUDA-core kernel); 'batch' = the ragged "
                          "batch with 64 subarrays; 'cc' = cross-correlation of the reference "
-                         "example's day (one JSON line)")
+                         "example's day (one JSON line); noise0, eq_short, small, cc_direct: "
+                         "see run_profile_extra")
     ap.add_argument("--config", type=int, default=0, choices=(0, 1, 3, 4, 5),
                     help="measure one other workload alone (one JSON line): 1 small noise array, "
                          "3 earthquake, 4 MWFJ, 5 ragged batch")
@@ -1314,6 +1375,8 @@ def main():
         return run_profile_mwfj(args)
     if args.profile_case == "cc":
         return run_cc_case(args)
+    if args.profile_case in ("noise0", "eq_short", "small", "cc_direct"):
+        return run_profile_extra(args)
     if args.profile_case == "batch":
         args.config = 5
         args.batch_small = True

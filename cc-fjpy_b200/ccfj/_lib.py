@@ -90,6 +90,8 @@ PROBE_SIGNATURES = {
                                          ctypes.POINTER(ctypes.c_double)]),
     "ccfj_special_device": (ctypes.c_int, [ctypes.c_int, ctypes.c_longlong, ctypes.c_void_p,
                                            ctypes.c_void_p, ctypes.c_void_p]),
+    "ccfj_paired_probe": (ctypes.c_int, [ctypes.c_longlong, ctypes.c_void_p, ctypes.c_void_p,
+                                         ctypes.c_void_p]),
 }
 
 _LIB = None

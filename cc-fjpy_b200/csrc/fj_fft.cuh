@@ -33,7 +33,7 @@ int rfft_bins(const FftJob& job, int nrows_out, cudaStream_t s, Scratch& sc);
 // MWFJ transform of all windows at once from their spectra
 // ([nwin][ntr][nf] complex, sorted traces), CUDA-core contraction.
 int mwfj_cuda_core(const ccfj_eq_args& a, const float2* spec, cudaStream_t s, Scratch& sc);
-// The same contraction on the tensor cores (tcgen05, BF16x3): itype 1,
+// The same contraction on the tensor cores (tcgen05, scaled FP16x3): itype 1,
 // func 0, 2 <= nr, nwin <= 128.
 // call_err: a device word for this call's timeout flag (NULL: taken from sc).
 int mwfj_tensor(const ccfj_eq_args& a, const float2* spec, cudaStream_t s, Scratch& sc,

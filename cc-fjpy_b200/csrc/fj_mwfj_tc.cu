@@ -11,10 +11,14 @@
 // k^2 (fj_earthquake's magnitude, src/ccfj-gpu.pyx:282-284) and the
 // per-frequency normalisation. A is generated on the fly (the station-
 // amortised FP32 special functions, one thread per velocity); B is the
-// windows' interval data, prepared once. Both are split into bf16 hi + lo
-// parts and the product is formed as A_hi B_hi + A_hi B_lo + A_lo B_hi
-// with FP32 accumulation in tensor memory (BF16x3, about 16 bits of
-// mantissa per operand).
+// windows' interval data, prepared once. Both are split into fp16 hi + lo
+// parts (22 bits of mantissa per operand) and the product is formed as
+// A_hi B_hi + A_hi B_lo + A_lo B_hi with FP32 accumulation in tensor memory
+// (FP16x3). fp16's range is kept by exact power-of-two scales: per row
+// (velocity) of A from a bound of its entries, per (frequency, window) of B
+// from the largest spectrum value, both undone in the epilogue; and the
+// slope column uses I1 / (k s) against the spectrum difference g2 - g1
+// (s = max(r2 - r1, 0.1), so that (I1 / k) b = (I1 / (k s)) (g2 - g1)).
 //
 // CTA: 256 threads = 256 velocities (two M = 128 accumulators), one
 // frequency, all windows (N = 2 nwin padded to a multiple of 16, <= 256).
@@ -24,7 +28,7 @@
 // chunks ahead), issues 12 tcgen05.mma and commits them to an mbarrier that
 // releases the stage. Two stages. All waits are bounded; a wait that runs
 // out sets an error flag, drains what is in flight and returns.
-#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <stdint.h>
 
 #include "fj_cells.cuh"
@@ -37,7 +41,7 @@ namespace tc {
 constexpr int kThreads = 256;       // velocities per CTA (2 x M = 128)
 constexpr int kChunkI = 16;         // intervals per chunk
 constexpr int kChunkK = 2 * kChunkI;  // K per chunk (I0 and I1/k per interval)
-constexpr int kSlices = kChunkK / 16;  // MMA K = 16 for bf16
+constexpr int kSlices = kChunkK / 16;  // MMA K = 16 for 16-bit operands
 constexpr int kSliceBytes128 = 128 * 16 * 2;  // one K-slice of a 128-row operand: 4096 B
 constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 2 GHz: a wait longer than this is an error
 
@@ -108,17 +112,17 @@ __device__ __forceinline__ uint64_t smem_desc(const void* p, uint32_t lbo, uint3
   return d;                // base offset 0, legacy LBO mode, SWIZZLE_NONE
 }
 
-// Instruction descriptor of kind::f16: BF16 A and B (K-major), F32 D.
-__host__ __device__ constexpr uint32_t instr_desc_bf16(int M, int N) {
+// Instruction descriptor of kind::f16: F16 A and B (K-major, format 0), F32 D.
+__host__ __device__ constexpr uint32_t instr_desc_f16(int M, int N) {
   return (1u << 4)                       // D format F32
-         | (1u << 7)                     // A format BF16
-         | (1u << 10)                    // B format BF16
+         | (0u << 7)                     // A format F16
+         | (0u << 10)                    // B format F16
          | ((uint32_t)(N >> 3) << 17)    // N / 8
          | ((uint32_t)(M >> 4) << 24);   // M / 16
 }
 
-__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc,
-                                         uint32_t accumulate) {
+__device__ __forceinline__ void mma_f16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc,
+                                        uint32_t accumulate) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
@@ -147,20 +151,40 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
 }
 
-// bf16 hi / lo split of v: hi = rn(v), lo = rn(v - hi).
-__device__ __forceinline__ void split_bf16(float v, __nv_bfloat16& hi, __nv_bfloat16& lo) {
-  hi = __float2bfloat16_rn(v);
-  lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+// fp16 hi / lo split of v: hi = rn(v), lo = rn(v - hi).
+__device__ __forceinline__ void split_f16(float v, __half& hi, __half& lo) {
+  hi = __float2half_rn(v);
+  lo = __float2half_rn(v - __half2float(hi));
+}
+
+// The same split of two values at once (the two K columns of one interval:
+// one packed conversion each for hi and lo, one paired subtraction).
+__device__ __forceinline__ void split_f16x2(float a, float b, __half2& hi, __half2& lo) {
+  hi = __floats2half2_rn(a, b);
+  const float2 h = __half22float2(hi);
+  lo = __floats2half2_rn(a - h.x, b - h.y);
+}
+
+// 2^(14 - e) for bound = m 2^e (m in [0.5, 1)): a value of magnitude <= bound
+// times it stays below 2^14 (fp16 holds up to 65504); 1 for a bound that is
+// zero or not finite; the exponent clamped to [-120, 120] (normal floats).
+__device__ __forceinline__ float pow2_scale_below_2_14(float bound) {
+  if (!(bound > 0.0f) || !isfinite(bound)) return 1.0f;
+  int e;
+  frexpf(bound, &e);
+  return ldexpf(1.0f, max(-120, min(120, 14 - e)));
 }
 
 }  // namespace tc
 
 struct MwTcDev {
   const float* rs;
-  const float* drs;         // [nr + 1]
   const uint4* bchunks;     // [nf][nchunks] chunks of (hi, lo) B tiles, chunk_bytes each
   const float* f;
   const float* c;
+  const float2* dinv;       // [nr + 1]: (r_i - r_{i-1}, 1 / max(r_i - r_{i-1}, 0.1))
+  const float* bounds;      // [2]: max |r|, max |r_i - r_{i-1}| (row scales of A)
+  const float* bscale;      // [nwin][nf]: power-of-two scale of B per (window, frequency)
   float* out;               // [nwin][nc][nf]
   unsigned int* err;        // this call's flag: set to 1 when a bounded wait runs out
   unsigned int* sticky;     // process-wide flag (g_mw_tc_error) set alongside, or NULL
@@ -174,8 +198,8 @@ struct MwTcDev {
 };
 
 // Shared-memory layout of one CTA (dynamic):
-//   A[stage][half m][hi/lo][slice] 128 rows x 16 K bf16   2*2*2*2*4096 = 64 KB
-//   B[stage][hi/lo][slice]         N rows x 16 K bf16     2*2*2*(N*32) B
+//   A[stage][half m][hi/lo][slice] 128 rows x 16 K fp16   2*2*2*2*4096 = 64 KB
+//   B[stage][hi/lo][slice]         N rows x 16 K fp16     2*2*2*(N*32) B
 //   barriers, tmem address
 struct TcSmem {
   static constexpr int kABytesStage = 2 * 2 * tc::kSlices * tc::kSliceBytes128;
@@ -238,7 +262,12 @@ __global__ void __launch_bounds__(tc::kThreads, 2) fj_mw_tc_kernel(MwTcDev a) {
   ZB<float> Yz{};
   Station<float> sp;
   float xp = cell.k * __ldg(a.rs);
-  float dr_next = __ldg(a.drs + 1);
+  float2 dn = __ldg(a.dinv + 1);
+  float dr_next = dn.x;
+  // this row's scale: |I0| and |I1 / (k s)| are at most max(1, sqrt(k rmax)) k Dmax
+  const float row_bound = fmaxf(1.0f, sqrtf(cell.k * __ldg(a.bounds))) * cell.k * __ldg(a.bounds + 1);
+  const float sa = tc::pow2_scale_below_2_14(row_bound);
+  const float c0s = sa, c1s = sa * cell.inv_k;  // scales of the two A columns (exact: sa = 2^m)
   cell.eval<true, false, true>(__ldg(a.rs), xp, closed_form<float, false>(cell.k * dr_next, xp, tau),
                                Jz, Yz);
   sp = fjs::make_station(xp, Jz);
@@ -246,7 +275,7 @@ __global__ void __launch_bounds__(tc::kThreads, 2) fj_mw_tc_kernel(MwTcDev a) {
 
   const int mh = tid >> 7;      // accumulator (M half)
   const int row = tid & 127;    // row inside it
-  const uint32_t idesc = tc::instr_desc_bf16(128, a.N);
+  const uint32_t idesc = tc::instr_desc_f16(128, a.N);
   int issued_b = a.self_test_no_copy ? 0 : (a.nchunks < 2 ? a.nchunks : 2);  // thread 0's count
   int committed = 0;                             // MMA groups committed (thread 0's count)
 
@@ -270,7 +299,7 @@ __global__ void __launch_bounds__(tc::kThreads, 2) fj_mw_tc_kernel(MwTcDev a) {
     unsigned char* aLo = aHi + tc::kSlices * tc::kSliceBytes128;
 #pragma unroll 1
     for (int j4 = 0; j4 < tc::kChunkI; j4 += 4) {
-      __nv_bfloat16 hi[8], lo[8];
+      __half2 hi[4], lo[4];
 #pragma unroll
       for (int jj = 0; jj < 4; ++jj) {
         const int i = 1 + kc * tc::kChunkI + j4 + jj;
@@ -278,7 +307,9 @@ __global__ void __launch_bounds__(tc::kThreads, 2) fj_mw_tc_kernel(MwTcDev a) {
         if (i < a.nr) {
           const float r = __ldg(a.rs + i);
           const float dr = dr_next;
-          dr_next = __ldg(a.drs + i + 1);
+          const float inv_s = dn.y;  // 1 / max(dr, 0.1)
+          dn = __ldg(a.dinv + i + 1);
+          dr_next = dn.x;
           const float x = cell.k * r;
           const float dx = cell.k * dr;
           const bool lc = ln;
@@ -289,10 +320,10 @@ __global__ void __launch_bounds__(tc::kThreads, 2) fj_mw_tc_kernel(MwTcDev a) {
           fjs::interval_moments<float>(sp, st, dx, lc, I0, I1);
           sp = st;
           xp = x;
-          I1k = I1 * cell.inv_k;
+          I0 *= c0s;
+          I1k = I1 * c1s * inv_s;
         }
-        tc::split_bf16(I0, hi[2 * jj], lo[2 * jj]);
-        tc::split_bf16(I1k, hi[2 * jj + 1], lo[2 * jj + 1]);
+        tc::split_f16x2(I0, I1k, hi[jj], lo[jj]);
       }
       const int off = tile_off(row, 2 * j4, 128);
       *reinterpret_cast<uint4*>(aHi + off) = *reinterpret_cast<const uint4*>(hi);
@@ -318,9 +349,9 @@ __global__ void __launch_bounds__(tc::kThreads, 2) fj_mw_tc_kernel(MwTcDev a) {
             const uint64_t dbh = tc::smem_desc(bHi + sl * a.N * 32, 128, 256);
             const uint64_t dbl = tc::smem_desc(bLo + sl * a.N * 32, 128, 256);
             const uint32_t acc0 = (kc > 0 || sl > 0) ? 1u : 0u;
-            tc::mma_bf16(d, dah, dbh, idesc, acc0);
-            tc::mma_bf16(d, dah, dbl, idesc, 1u);
-            tc::mma_bf16(d, dal, dbh, idesc, 1u);
+            tc::mma_f16(d, dah, dbh, idesc, acc0);
+            tc::mma_f16(d, dah, dbl, idesc, 1u);
+            tc::mma_f16(d, dal, dbh, idesc, 1u);
           }
         }
         tc::mma_commit(bar + 2 + s);
@@ -356,6 +387,7 @@ __global__ void __launch_bounds__(tc::kThreads, 2) fj_mw_tc_kernel(MwTcDev a) {
     // epilogue: row `row` of accumulator `mh` -> |Re + i Im| / k^2
     const uint32_t tbase = tmem + ((uint32_t)(tid & 96) << 16) + (uint32_t)(mh * a.N);
     const int c = c0 + tid;
+    const float inv_sa = 1.0f / sa;  // exact: a power of two
     for (int col = 0; col < a.N; col += 16) {
       float v[16];
       tc::tmem_ld16(tbase + (uint32_t)col, v);
@@ -364,7 +396,10 @@ __global__ void __launch_bounds__(tc::kThreads, 2) fj_mw_tc_kernel(MwTcDev a) {
         for (int j = 0; j < 16; j += 2) {
           const int w = (col + j) >> 1;
           if (w < a.nwin) {
-            const float re = v[j] * cell.inv_k2, im = v[j + 1] * cell.inv_k2;
+            const float inv_sb = 1.0f / __ldg(a.bscale + (long long)w * a.nf + fi);
+            // the scales are powers of two: undoing them is exact
+            const float re = v[j] * inv_sa * inv_sb * cell.inv_k2;
+            const float im = v[j + 1] * inv_sa * inv_sb * cell.inv_k2;
             a.out[((long long)w * a.nc + c) * a.nf + fi] = sqrtf(re * re + im * im);
           }
         }
@@ -383,16 +418,19 @@ __global__ void __launch_bounds__(tc::kThreads, 2) fj_mw_tc_kernel(MwTcDev a) {
 }
 
 // The B operand of every (frequency, chunk of 16 intervals): window w's
-// interval data (g_{i-1}, b_i) of its real (row 2w) and imaginary (row 2w+1)
-// part, split into bf16 hi and lo, in the tensor cores' K-major tile layout.
-// One CTA builds the tiles of kPrepF consecutive frequencies and one chunk
-// in shared memory -- reading each (window, interval) for those frequencies
-// as one 32-byte piece -- then stores each frequency's tile contiguously.
-// Rows past the last window and intervals past the last pair are zero.
+// interval data of its real (row 2w) and imaginary (row 2w+1) part --
+// g_{i-1} and the difference g_i - g_{i-1} (the slope b_i times
+// s_i = max(r_i - r_{i-1}, 0.1), src/FJcpu.cpp:259-261; A carries 1 / s_i) --
+// times the (window, frequency) scale, split into fp16 hi and lo, in the
+// tensor cores' K-major tile layout. One CTA builds the tiles of kPrepF
+// consecutive frequencies and one chunk in shared memory -- reading each
+// (window, interval) for those frequencies as one 32-byte piece -- then
+// stores each frequency's tile contiguously. Rows past the last window and
+// intervals past the last pair are zero.
 constexpr int kPrepF = 4;
 __global__ void __launch_bounds__(256) mw_tc_prep_kernel(const float2* __restrict__ spec, int ntr,
                                                          int nf, int nwin, int N, int nchunks,
-                                                         const float* __restrict__ drs,
+                                                         const float* __restrict__ bscale,
                                                          unsigned char* __restrict__ dst) {
   extern __shared__ uint4 tile_u4[];
   unsigned char* tile = reinterpret_cast<unsigned char*>(tile_u4);
@@ -408,31 +446,31 @@ __global__ void __launch_bounds__(256) mw_tc_prep_kernel(const float2* __restric
     const int jj = t / (kPrepF * nw2);
     const int i = 1 + kc * tc::kChunkI + jj;  // interval i: pairs i-1, i
     const int fi = f0 + f;
-    float g0r = 0.f, br = 0.f, g0i = 0.f, bi = 0.f;
+    float g0r = 0.f, dr = 0.f, g0i = 0.f, di = 0.f;
     if (w < nwin && i < ntr && fi < nf) {
       const float2 cur = spec[((long long)w * ntr + i) * nf + fi];
       const float2 prv = spec[((long long)w * ntr + i - 1) * nf + fi];
-      const float d = fmaxf(drs[i], 0.1f);  // src/FJcpu.cpp:259-261
-      g0r = prv.x;
-      br = (cur.x - prv.x) / d;
-      g0i = prv.y;
-      bi = (cur.y - prv.y) / d;
+      const float sb = bscale[(long long)w * nf + fi];  // a power of two: exact
+      g0r = prv.x * sb;
+      dr = (cur.x - prv.x) * sb;
+      g0i = prv.y * sb;
+      di = (cur.y - prv.y) * sb;
     }
     unsigned char* base = tile + (long long)f * chunk_bytes;
-    const float g0v[2] = {g0r, g0i}, bv[2] = {br, bi};
+    const float g0v[2] = {g0r, g0i}, dv[2] = {dr, di};
 #pragma unroll
     for (int part = 0; part < 2; ++part) {
-      __nv_bfloat16 h0, l0, h1, l1;
-      tc::split_bf16(g0v[part], h0, l0);
-      tc::split_bf16(bv[part], h1, l1);
-      __nv_bfloat162 hh, ll;
+      __half h0, l0, h1, l1;
+      tc::split_f16(g0v[part], h0, l0);
+      tc::split_f16(dv[part], h1, l1);
+      __half2 hh, ll;
       hh.x = h0;
       hh.y = h1;
       ll.x = l0;
       ll.y = l1;
       const int off = tile_off(2 * w + part, 2 * jj, N);
-      *reinterpret_cast<__nv_bfloat162*>(base + off) = hh;
-      *reinterpret_cast<__nv_bfloat162*>(base + half + off) = ll;
+      *reinterpret_cast<__half2*>(base + off) = hh;
+      *reinterpret_cast<__half2*>(base + half + off) = ll;
     }
   }
   __syncthreads();
@@ -442,6 +480,67 @@ __global__ void __launch_bounds__(256) mw_tc_prep_kernel(const float2* __restric
     if (f0 + f < nf)
       reinterpret_cast<uint4*>(dst + ((long long)(f0 + f) * nchunks + kc) * chunk_bytes)[q] =
           tile_u4[f * per_f + q];
+  }
+}
+
+// (r_i - r_{i-1}, 1 / max(r_i - r_{i-1}, 0.1)) per interval from drs.
+__global__ void mw_tc_dinv_kernel(const float* __restrict__ drs, int n, float2* __restrict__ dinv) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dinv[i] = make_float2(drs[i], 1.0f / fmaxf(drs[i], 0.1f));
+}
+
+// max |r| and max |r_i - r_{i-1}| (one CTA of 1024 threads).
+__global__ void __launch_bounds__(1024) mw_tc_bounds_kernel(const float* __restrict__ rs,
+                                                            const float* __restrict__ drs, int nr,
+                                                            float* __restrict__ out) {
+  __shared__ float red[2][32];
+  float mr = 0.f, md = 0.f;
+  for (int i = threadIdx.x; i <= nr; i += blockDim.x) {
+    if (i < nr) mr = fmaxf(mr, fabsf(rs[i]));
+    md = fmaxf(md, fabsf(drs[i]));
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    mr = fmaxf(mr, __shfl_xor_sync(0xffffffffu, mr, o));
+    md = fmaxf(md, __shfl_xor_sync(0xffffffffu, md, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = mr;
+    red[1][threadIdx.x >> 5] = md;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    mr = threadIdx.x < (blockDim.x >> 5) ? red[0][threadIdx.x] : 0.f;
+    md = threadIdx.x < (blockDim.x >> 5) ? red[1][threadIdx.x] : 0.f;
+    for (int o = 16; o > 0; o >>= 1) {
+      mr = fmaxf(mr, __shfl_xor_sync(0xffffffffu, mr, o));
+      md = fmaxf(md, __shfl_xor_sync(0xffffffffu, md, o));
+    }
+    if (threadIdx.x == 0) {
+      out[0] = mr;
+      out[1] = md;
+    }
+  }
+}
+
+// Per (window, frequency): the power-of-two scale that keeps the window's
+// B entries (spectrum values and differences of neighbours, at most twice
+// the largest |Re| or |Im| over the traces) below 2^14.
+__global__ void mw_tc_bscale_kernel(const float2* __restrict__ spec, int ntr, int nf,
+                                    float* __restrict__ bscale) {
+  __shared__ float red[8][33];
+  const int fi = blockIdx.x * 32 + threadIdx.x;
+  const int w = blockIdx.y;
+  float m = 0.f;
+  if (fi < nf)
+    for (int i = threadIdx.y; i < ntr; i += 8) {
+      const float2 v = spec[((long long)w * ntr + i) * nf + fi];
+      m = fmaxf(m, fmaxf(fabsf(v.x), fabsf(v.y)));
+    }
+  red[threadIdx.y][threadIdx.x] = m;
+  __syncthreads();
+  if (threadIdx.y == 0 && fi < nf) {
+    for (int y = 1; y < 8; ++y) m = fmaxf(m, red[y][threadIdx.x]);
+    bscale[(long long)w * nf + fi] = tc::pow2_scale_below_2_14(2.0f * m);
   }
 }
 
@@ -470,12 +569,25 @@ int mwfj_tensor(const ccfj_eq_args& a, const float2* spec, cudaStream_t s, Scrat
   const int nchunks = (nr - 1 + tc::kChunkI - 1) / tc::kChunkI;
   const long long chunk_bytes = 2LL * tc::kSlices * N * 32;
   unsigned char* bch = static_cast<unsigned char*>(sc.get((size_t)nf * nchunks * chunk_bytes));
-  if (!bch) return CCFJ_ERR_ALLOC;
+  float2* dinv = sc.get_n<float2>(nr + 1);
+  float* bounds = sc.get_n<float>(2);
+  float* bscale = sc.get_n<float>((size_t)nwin * nf);
+  if (!bch || !dinv || !bounds || !bscale) return CCFJ_ERR_ALLOC;
+  CCFJ_REQUIRE(nwin <= 65535, "MWFJ tensor path: nwin=%d", nwin);
+  mw_tc_dinv_kernel<<<div_up(nr + 1, 256), 256, 0, s>>>(drs, nr + 1, dinv);
+  count_launch();
+  CCFJ_LAUNCH_CHECK("mw_tc_dinv_kernel");
+  mw_tc_bounds_kernel<<<1, 1024, 0, s>>>(a.r, drs, nr, bounds);
+  count_launch();
+  CCFJ_LAUNCH_CHECK("mw_tc_bounds_kernel");
+  mw_tc_bscale_kernel<<<dim3(div_up(nf, 32), nwin), dim3(32, 8), 0, s>>>(spec, nr, nf, bscale);
+  count_launch();
+  CCFJ_LAUNCH_CHECK("mw_tc_bscale_kernel");
   const size_t prep_smem = (size_t)kPrepF * chunk_bytes;
   CCFJ_CUDA_TRY(cudaFuncSetAttribute(mw_tc_prep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)prep_smem));
   mw_tc_prep_kernel<<<dim3(nchunks, div_up(nf, kPrepF)), 256, prep_smem, s>>>(
-      spec, nr, nf, nwin, N, nchunks, drs, bch);
+      spec, nr, nf, nwin, N, nchunks, bscale, bch);
   count_launch();
   CCFJ_LAUNCH_CHECK("mw_tc_prep_kernel");
   unsigned int* sticky = nullptr;
@@ -485,7 +597,9 @@ int mwfj_tensor(const ccfj_eq_args& a, const float2* spec, cudaStream_t s, Scrat
   CCFJ_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(unsigned int), s));
   MwTcDev d{};
   d.rs = a.r;
-  d.drs = drs;
+  d.dinv = dinv;
+  d.bounds = bounds;
+  d.bscale = bscale;
   d.bchunks = reinterpret_cast<const uint4*>(bch);
   d.f = a.f;
   d.c = a.c;
@@ -533,11 +647,21 @@ int mw_tc_self_test(cudaStream_t s, int* status) {
   float* wtr = sc.get_n<float>(nr);
   unsigned int* err = sc.get_n<unsigned int>(1);
   if (!wtr || !err) return CCFJ_ERR_ALLOC;
+  float2* dinv = sc.get_n<float2>(nr + 1);
+  float* bounds = sc.get_n<float>(2);
+  float* bscale = sc.get_n<float>(1);
+  if (!dinv || !bounds || !bscale) return CCFJ_ERR_ALLOC;
   fj_prep_geom_kernel_shared(r, nr, drs, wtr, s);
+  mw_tc_dinv_kernel<<<1, 32, 0, s>>>(drs, nr + 1, dinv);
+  mw_tc_bounds_kernel<<<1, 1024, 0, s>>>(r, drs, nr, bounds);
+  const float one = 1.0f;
+  CCFJ_CUDA_TRY(cudaMemcpyAsync(bscale, &one, sizeof(one), cudaMemcpyHostToDevice, s));
   CCFJ_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(unsigned int), s));
   MwTcDev d{};
   d.rs = r;
-  d.drs = drs;
+  d.dinv = dinv;
+  d.bounds = bounds;
+  d.bscale = bscale;
   d.bchunks = reinterpret_cast<const uint4*>(bch);
   d.f = fc;
   d.c = fc + 1;

@@ -230,7 +230,8 @@ typedef struct ccfj_eq_args {
 
 CCFJ_API int ccfj_fj_earthquake_v1(const ccfj_eq_args *args, void *stream);
 /* MWFJ contraction of the windows: 0 = automatic (tensor cores, tcgen05
- * BF16x3 with FP32 accumulation, for itype 1, func 0 and 8 <= nwin <= 128;
+ * FP16x3 (hi/lo fp16 operands with exact power-of-two scales) with FP32
+ * accumulation, for itype 1, func 0 and 8 <= nwin <= 128;
  * CUDA-core FMAs otherwise), 1 = always CUDA cores, 2 = tensor cores
  * wherever supported. */
 CCFJ_API int ccfj_set_mwfj_path(int path);

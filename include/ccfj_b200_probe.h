@@ -27,4 +27,12 @@ CCFJ_PROBE_API int ccfj_special_host(int precision, long long n, const double *x
 CCFJ_PROBE_API int ccfj_special_device(int precision, long long n, const double *x, double *out,
                                        void *stream);
 
+/* The transform kernels' station values y0 = J0 / M, y1 = J1 / M of two
+ * cells (f, c0) and (f, c1) at distance r, x = 2 pi f r / c >= 8 in both:
+ * in[4*i .. 4*i+3] = f, c0, c1, r (device pointer, float32); out[8*i ..]
+ * = the scalar path's y0, y1 of cell 0 and of cell 1, then the paired path's
+ * (two cells per FFMA2 / FMUL2 / FADD2) in the same order. Async on stream.
+ * Returns 0, 1 (invalid argument), 2 (launch failed) or 4 (not sm_100). */
+CCFJ_PROBE_API int ccfj_paired_probe(long long n, const float *in, float *out, void *stream);
+
 #endif /* CCFJ_B200_PROBE_H */

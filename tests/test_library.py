@@ -30,7 +30,7 @@ def test_library_exports_every_declared_symbol(lib):
 def test_probe_library_is_separate(lib, probe):
     """The special-function probes live in the test library only."""
     syms = declared_symbols("ccfj_b200_probe.h", "CCFJ_PROBE_API")
-    assert set(syms) == {"ccfj_special_host", "ccfj_special_device"}
+    assert set(syms) == {"ccfj_special_host", "ccfj_special_device", "ccfj_paired_probe"}
     for name in syms:
         assert hasattr(probe, name), name
     import subprocess

@@ -86,3 +86,30 @@ def test_device_functions(probe, prec, tol):
         else:
             err = np.abs(got[:, j] - REF[:, j]) / scale
             assert err.max() < tol, (name, err.max(), XS[err.argmax()])
+
+
+@pytest.mark.gpu
+def test_paired_station_values_equal_scalar(probe):
+    """The paired (two cells per FFMA2 / FMUL2 / FADD2) x >= 8 evaluation of
+    the transform kernels against their scalar one: the same values, cell by
+    cell, over the frequencies, velocities and distances of the benchmark
+    workloads."""
+    import torch
+    rng = np.random.default_rng(3)
+    n = 200000
+    f = rng.uniform(0.005, 2.0, n)
+    c0 = rng.uniform(500.0, 5000.0, n)
+    c1 = c0 + rng.choice([4.5, 1.75, 224.0], n)
+    r = rng.uniform(1e3, 1.5e6, n)
+    x = 2 * np.pi * f * r / np.maximum(c0, c1)
+    keep = x >= 8.5
+    inp = np.stack([f, c0, c1, r], axis=1)[keep].astype(np.float32)
+    d_in = torch.from_numpy(np.ascontiguousarray(inp)).cuda()
+    d_out = torch.zeros((len(inp), 8), dtype=torch.float32, device="cuda")
+    st = probe.ccfj_paired_probe(len(inp), ctypes.c_void_p(d_in.data_ptr()),
+                                 ctypes.c_void_p(d_out.data_ptr()), None)
+    assert st == 0
+    o = d_out.cpu().numpy()
+    scalar, paired = o[:, :4], o[:, 4:]
+    diff = np.abs(scalar - paired)
+    assert diff.max() <= 2e-6, (diff.max(), inp[diff.max(axis=1).argmax()])
