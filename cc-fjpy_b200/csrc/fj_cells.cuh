@@ -660,7 +660,7 @@ __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
     for (int o = 16; o > 0; o >>= 1) s8w = fmax(s8w, __shfl_xor_sync(0xffffffffu, s8w, o));
     // Paired FP32 arithmetic (two cells per FFMA2 / FMUL2 / FADD2) for the
     // J-basis modes with an even number of cells per thread; the Y basis
-    // and the explicit path stay scalar. Bitwise the scalar result.
+    // and the explicit path stay scalar.
 #ifndef CCFJ_PAIRED
 #define CCFJ_PAIRED 1
 #endif

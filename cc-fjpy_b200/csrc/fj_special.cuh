@@ -440,8 +440,9 @@ FJ_HD void eval_station_f64(double x, double t, ZB<double>& J, ZB<double>& Y) {
 // instruction (FFMA2 / FMUL2 / FADD2 on sm_100). Each lane performs exactly
 // the scalar function's operations in the same order with the same
 // rounding -- negated quantities come from negated inputs or coefficients,
-// which round-to-nearest maps to exactly negated results -- so the pair
-// equals two scalar calls bit for bit, with about half the instructions.
+// which round-to-nearest maps to exactly negated results -- with about half
+// the instructions; tests/test_special_host.py holds it to the scalar path
+// on the device.
 #if defined(__CUDACC__)
 #if !defined(__CUDA_ARCH__) || __CUDA_ARCH__ >= 1000
 #define FJS_HAVE_PAIRED 1
@@ -482,10 +483,16 @@ __device__ __forceinline__ void eval_large_scaled_pair_j(const PairPhase& ph, fl
                                                          ZB2& J) {
   const float2 rr = psplat(r);
   // p_hi + p_lo = q r (the scalar: p_hi = q_hi r, e = fma(q_hi, r, -p_hi),
-  // p_lo = fma(q_lo, r, e))
+  // p_lo = fma(q_lo, r, e)). The rounding error e of q_hi r is formed by
+  // one fused multiply-add per lane in inline PTX, which the compiler can
+  // neither split nor fold with the product it cancels: measured, the
+  // paired form of that step lost e (about 2e-3 rad of phase at x = 3e4).
   const float2 p_hi = pmul(ph.qhi, rr);
   const float2 np_hi = pmul(ph.nqhi, rr);  // -p_hi exactly
-  const float2 p_lo = pfma(ph.qlo, rr, pfma(ph.qhi, rr, np_hi));
+  float2 e;
+  asm("fma.rn.f32 %0, %1, %2, %3;" : "=f"(e.x) : "f"(ph.qhi.x), "f"(r), "f"(np_hi.x));
+  asm("fma.rn.f32 %0, %1, %2, %3;" : "=f"(e.y) : "f"(ph.qhi.y), "f"(r), "f"(np_hi.y));
+  const float2 p_lo = pfma(ph.qlo, rr, e);
   // chi_cycles_f32: (p_hi - n) + (p_lo - 1/8), n = (p_hi + 1.5 2^23) - 1.5 2^23;
   // -n = (-p_hi - 1.5 2^23) + 1.5 2^23 exactly
   const float kMagic = 12582912.0f;
