@@ -493,6 +493,13 @@ def measure_small(lib, torch, dev, sp, peak, args):
     a = _fj_args(nr, nf, nc, 1, _lib.MODE_J, d["u"].data_ptr(), 2 * nf, 2, None, d["r"], d["f"],
                  d["c"], out)
     fn = lambda: _lib.check(lib.ccfj_fj_v1(ctypes.byref(a), sp))  # noqa: E731
+    # the tile choice (velocities per thread x station ranges) from the
+    # project's autotuner, recorded for this problem class before timing
+    best, best_ms = ctypes.c_int(), ctypes.c_float()
+    _lib.check(lib.ccfj_autotune_fj_v1(ctypes.byref(a), sp, ctypes.byref(best),
+                                       ctypes.byref(best_ms)))
+    cpt, nsplit = ctypes.c_int(), ctypes.c_int()
+    _lib.check(lib.ccfj_tuned_choice_fj(ctypes.byref(a), ctypes.byref(cpt), ctypes.byref(nsplit)))
     s, ks, launches, clocks = _time_profiled(lib, fn, 200, 10, dev)
     y32 = out.cpu().numpy()
     a.precision = _lib.PREC_FP64
@@ -505,6 +512,9 @@ def measure_small(lib, torch, dev, sp, peak, args):
                     "300 c (1000-5000 m/s), sigma 0.1", "unit": "terms/s",
         "value": terms / s, "ms_per_call": s * 1e3, "gpu_launches_per_call": launches,
         "clocks": clocks,
+        "tile_choice": {"velocities_per_thread": cpt.value, "station_ranges": nsplit.value,
+                        "source": "ccfj_autotune_fj_v1 (best of 1/2/4 velocities per thread x "
+                                  "1-8 station ranges, %.3f ms)" % best_ms.value},
         "e2e": {"value": terms / te, "unit": "terms/s", "ms_per_call": te * 1e3,
                 "h2d_bytes_per_step": int(uf.nbytes + r.nbytes + 8 * nr + 4 * (nf + nc)),
                 "d2h_bytes_per_step": int(ye.nbytes)},

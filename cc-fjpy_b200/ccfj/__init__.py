@@ -235,5 +235,6 @@ from ._eq import fj_earthquake, MWFJ  # noqa: E402
 from ._batch import fj_noise_batch  # noqa: E402
 from ._cc import CC, cc_fj_noise  # noqa: E402
 from ._io import load_ncfs, pinned_empty  # noqa: E402
+from ._pick import pick_curve  # noqa: E402
 from ._shims import CC_full, fH_full, fHi_full, fHr_full, fj_full  # noqa: E402
 from . import dist  # noqa: E402,F401

@@ -481,26 +481,21 @@ struct PairPhase {
 // the station r (1/r = rinv): y0 = J0 / M and y1 = J1 / M, x >= 8 in both.
 __device__ __forceinline__ void eval_large_scaled_pair_j(const PairPhase& ph, float r, float rinv,
                                                          ZB2& J) {
-  const float2 rr = psplat(r);
-  // p_hi + p_lo = q r (the scalar: p_hi = q_hi r, e = fma(q_hi, r, -p_hi),
-  // p_lo = fma(q_lo, r, e)). The rounding error e of q_hi r is formed by
-  // one fused multiply-add per lane in inline PTX, which the compiler can
-  // neither split nor fold with the product it cancels: measured, the
-  // paired form of that step lost e (about 2e-3 rad of phase at x = 3e4).
-  const float2 p_hi = pmul(ph.qhi, rr);
-  const float2 np_hi = pmul(ph.nqhi, rr);  // -p_hi exactly
-  float2 e;
-  asm("fma.rn.f32 %0, %1, %2, %3;" : "=f"(e.x) : "f"(ph.qhi.x), "f"(r), "f"(np_hi.x));
-  asm("fma.rn.f32 %0, %1, %2, %3;" : "=f"(e.y) : "f"(ph.qhi.y), "f"(r), "f"(np_hi.y));
-  const float2 p_lo = pfma(ph.qlo, rr, e);
-  // chi_cycles_f32: (p_hi - n) + (p_lo - 1/8), n = (p_hi + 1.5 2^23) - 1.5 2^23;
-  // -n = (-p_hi - 1.5 2^23) + 1.5 2^23 exactly
-  const float kMagic = 12582912.0f;
-  const float2 nn = padd(padd(np_hi, psplat(-kMagic)), psplat(kMagic));
-  const float2 u = padd(padd(p_hi, nn), padd(p_lo, psplat(-0.125f)));
+  // The phase in cycles, per lane with the scalar code (p_hi = q_hi r,
+  // p_lo = fma(q_lo, r, fma(q_hi, r, -p_hi)), chi_cycles_f32): written with
+  // paired operations it measured about 2e-3 rad less accurate at x = 3e4,
+  // as if the low part of the double-float phase had been lost.
   float2 sn, cs;
-  sincos_cycles_f32(u.x, sn.x, cs.x);
-  sincos_cycles_f32(u.y, sn.y, cs.y);
+  {
+    const float p_hi = ph.qhi.x * r;
+    const float p_lo = fmaf(ph.qlo.x, r, fmaf(ph.qhi.x, r, -p_hi));
+    sincos_cycles_f32(chi_cycles_f32(p_hi, p_lo), sn.x, cs.x);
+  }
+  {
+    const float p_hi = ph.qhi.y * r;
+    const float p_lo = fmaf(ph.qlo.y, r, fmaf(ph.qhi.y, r, -p_hi));
+    sincos_cycles_f32(chi_cycles_f32(p_hi, p_lo), sn.y, cs.y);
+  }
   const float2 sv = pmul(ph.s8, psplat(rinv));  // s = 8 / x
   const float2 z = pmul(sv, sv);
   constexpr float cp0[] = FJC_F32_L_P0;

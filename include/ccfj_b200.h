@@ -337,6 +337,21 @@ CCFJ_API int CrossCorrelation(ccfj_cc_data data);
  *   cross-spectra to the host between the two steps. */
 CCFJ_API int ccfj_cc_fj_noise_v1(const ccfj_cc_args *cc, const ccfj_fj_args *fj, void *stream);
 
+/* ------------------------------------------------- dispersion-curve picking
+ * Per frequency column of a spectrum spec[nc][nf] (e.g. a normalised F-J
+ * spectrum): the velocity of the first largest value among the velocities
+ * c[j] within [cmin[i], cmax[i]] (NULL: no bound), refined between the grid
+ * velocities by the vertex of the parabola through the maximum and its two
+ * neighbours (when both lie in the band and the parabola opens downward;
+ * the offset limited to half a grid step), into cpick[nf], and that
+ * vertex's value into amp[nf] (amp may be NULL). A column with a NaN in the
+ * band, or with no velocity in it, gives NaN. device_ptrs as in
+ * ccfj_fj_args. No counterpart in the reference, whose users pick curves
+ * from the plotted spectrum. */
+CCFJ_API int ccfj_pick_v1(const float *spec, int nc, int nf, const float *c, const float *cmin,
+                          const float *cmax, float *cpick, float *amp, int device_ptrs,
+                          void *stream);
+
 /* ------------------------------------------------------------- tuning
  * Tile choices of the FP32 transform: 1, 2 or 4 velocities per thread, and
  * the number of station ranges (split launch: ranges of whole 32-station
