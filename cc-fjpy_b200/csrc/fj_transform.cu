@@ -332,7 +332,10 @@ static int split_for(const ccfj_fj_args& a, int cpt, int split_choice) {
   if (forced > 0) return forced;
   const int tuned = tuned_split(a);
   if (tuned > 0) return tuned;
-  const long long ctas = (long long)div_up(a.nc, 8 * cpt) * div_up(a.nf, 32);
+  // a window of frequencies (col_begin, nf_total) decides as its whole
+  // problem does, so that windows reproduce the full transform
+  const int nf_all = a.nf_total > 0 ? a.nf_total : a.nf;
+  const long long ctas = (long long)div_up(a.nc, 8 * cpt) * div_up(nf_all, 32);
   const long long slots = (long long)sm_count() * CCFJ_FJ_MIN_BLOCKS;
   int n = 1;
   for (int k = 2; k <= 4; ++k)
@@ -661,6 +664,8 @@ static int fj_host_blocks(const ccfj_fj_args& a, cudaStream_t s, int nblk, int n
   // one call at a time per device uses the staging buffers
   std::lock_guard<std::mutex> pipe_lock(hp->use);
   cudaStream_t hs[2] = {hp->st[0], hp->st[1]};
+  const int full_cpt = variant_for(a, 0);
+  const int full_split = a.precision == CCFJ_PREC_FP32 ? split_for(a, full_cpt, 0) : 1;
   Scratch sc(s);
   float* dr = sc.get_n<float>(a.nr);
   float* df = sc.get_n<float>(a.nf);
@@ -798,7 +803,9 @@ static int fj_host_blocks(const ccfj_fj_args& a, cudaStream_t s, int nblk, int n
     d.c = dc;
     d.perm = dp;
     d.out = B.dout;
-    st = fj_device(d, cs);
+    // every block runs the whole problem's tile choice, so the blocks give
+    // the device path's result bit for bit
+    st = fj_device(d, cs, full_cpt, full_split);
     if (st != CCFJ_OK) return fail(st);
   }
   for (int p = 0; p < nblk; ++p) {

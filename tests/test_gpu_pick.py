@@ -61,5 +61,5 @@ def test_pick_edges():
     assert cp[1] == 2000.0 and amp[1] == 1.0
     assert np.isnan(cp[2]) and np.isnan(amp[2])
     assert cp[3] == 1000.0
-    cp, _ = ccfj.pick_curve(spec, c, cmin=1200.0, cmax=1250.0)   # no velocity in the band
+    cp, _ = ccfj.pick_curve(spec, c, cmin=1210.0, cmax=1250.0)   # no velocity in the band
     assert np.all(np.isnan(cp))
