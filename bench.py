@@ -519,8 +519,9 @@ def measure_small(lib, torch, dev, sp, peak, args):
                 "h2d_bytes_per_step": int(uf.nbytes + r.nbytes + 8 * nr + 4 * (nf + nc)),
                 "d2h_bytes_per_step": int(ye.nbytes)},
         "roofline": _fp32_roofline(FLOPS_PER_TERM_ITYPE1 * terms, ks, peak,
-                                   "fj_amortized_kernel<MODE_J, 1, float, 2>",
-                                   FLOPS_PER_TERM_ITYPE1),
+                                   "fj_amortized_kernel<MODE_J, 1, float, %d>" % cpt.value,
+                                   FLOPS_PER_TERM_ITYPE1,
+                                   traffic=profile_traffic("fj_split_small_array.md")),
         "accuracy": {"max_abs_err_vs_fp64_normalised": _err(y32, y64),
                      "nan_positions_equal_fp64": _nan_equal(y32, y64),
                      "fp64_sample": "all 300 x 512 cells", "e2e_equals_device": bool(
@@ -1281,8 +1282,31 @@ def run_cc_case(args):
     peak = ctypes.c_double(0)
     _lib.check(lib.ccfj_fp32_peak_probe(sp, ctypes.byref(peak)))
     tflops = (fft_flops + pair_flops) / dev_s / 1e12
+    # records to dispersion spectrum in one call (the cross-spectra stay on
+    # the device): station coordinates in a 300 x 300 km box, bins at
+    # fstride 3 of one-hour windows, 1000 velocities over 2000-5000 m/s (the
+    # reference's noise example), itype 1, func 0; host arrays in and out
+    xy = np.random.default_rng(8).uniform(0.0, 3e5, (nsta, 2))
+    pp = pairs.reshape(-1, 2)
+    r = np.hypot(*(xy[pp[:, 0]] - xy[pp[:, 1]]).T)
+    fbin = np.arange(nf) * fstride * fs / fftlen
+    fbin[0] = fbin[1] / 2  # keep k > 0 in the first column
+    cv = np.linspace(2000.0, 5000.0, 1000)
+    for _ in range(args.warmup):
+        ccfj.cc_fj_noise(npts, nsta, nf, fftlen, pairs, se, data, r, cv, fbin, overlaprate=overlap,
+                         fstride=fstride)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ccfj.cc_fj_noise(npts, nsta, nf, fftlen, pairs, se, data, r, cv, fbin, overlaprate=overlap,
+                         fstride=fstride)
+    chain_s = (time.perf_counter() - t0) / args.steps
     print(json.dumps({
         "case": "cc", "unit": "ms per call", "device_ms": dev_s * 1e3, "e2e_ms": e2e_s * 1e3,
+        "records_to_spectrum_ms": chain_s * 1e3,
+        "records_to_spectrum": "ccfj.cc_fj_noise on host arrays: the CC above, then fj_noise "
+                               "itype 1 func 0 on its %d pairs x %d bins x 1000 velocities; records "
+                               "in once (%.0f MB), spectrum out once (%.1f MB)" % (
+                                   npairs, nf, data.nbytes / 1e6, 4e-6 * nf * 1000),
         "gpu_launches_per_call": int(launches),
         "algorithmic_tflops": tflops, "fp32_peak_tflops": peak.value,
         "frac_fp32": tflops / peak.value,
