@@ -311,7 +311,8 @@ static int variant_for(const ccfj_fj_args& a, int cpt) {
 // given, else the tuned choice for the problem class, else enough ranges
 // that the grid fills the SMs' resident slots when the (velocity tile x
 // frequency tile) grid alone leaves them idle -- the largest n <= 4 with
-// n x CTAs <= 1.1 x slots and ranges of at least two station chunks.
+// n x CTAs <= slots (one more CTA would start a second wave) and ranges of
+// at least two station chunks.
 constexpr int kSplitAlign = 32;  // multiple of every staged chunk (16 or 32 stations)
 static int sm_count() {
   static std::atomic<int> cached{0};
@@ -339,7 +340,7 @@ static int split_for(const ccfj_fj_args& a, int cpt, int split_choice) {
   const long long slots = (long long)sm_count() * CCFJ_FJ_MIN_BLOCKS;
   int n = 1;
   for (int k = 2; k <= 4; ++k)
-    if (k * ctas * 10 <= slots * 11 && a.nr >= 2 * kSplitAlign * k) n = k;
+    if (k * ctas <= slots && a.nr >= 2 * kSplitAlign * k) n = k;
   return n;
 }
 
