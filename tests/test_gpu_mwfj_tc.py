@@ -1,4 +1,4 @@
-"""MWFJ's window contraction on the tensor cores (tcgen05, BF16x3) against
+"""MWFJ's window contraction on the tensor cores (tcgen05, scaled FP16x3) against
 the CUDA-core path and the FP64 oracle."""
 import ctypes
 import warnings

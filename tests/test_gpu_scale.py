@@ -7,7 +7,7 @@ workloads themselves through the public API and check
     samples, 1024 bins x 800 c) against the FP64 oracle, and against the
     reference's own FJcpu.cpp where its CPU build (make -C oracle) is present;
   * every window of the MWFJ workload (1000 traces x 16384 samples, 64
-    windows, 1024 bins x 2000 c; tensor cores, BF16x3) against the FP64 GPU
+    windows, 1024 bins x 2000 c; tensor cores, scaled FP16x3) against the FP64 GPU
     form, and two (window, bin) columns against the oracle;
   * every subarray of a 64-subarray ragged batch against the FP64 GPU form.
 Every frequency column is independent of the others (its normalisation
@@ -95,7 +95,7 @@ def test_earthquake_columns(pool):
 
 
 def test_mwfj_every_window(pool):
-    """BF16x3 tensor-core MWFJ: all 64 windows against the FP64 form."""
+    """Scaled FP16x3 tensor-core MWFJ: all 64 windows against the FP64 form."""
     import ccfj
     from ccfj import _eq, _lib
     b = _bench()
