@@ -690,8 +690,9 @@ def measure_mwfj(lib, torch, dev, sp, peak, bf16, args):
         "e2e": {"value": terms / te, "unit": "window terms/s", "ms_per_call": te * 1e3,
                 "h2d_bytes_per_step": int(u.nbytes + 12 * n1.size + 12 * ntr + 4 * (nf + nc)),
                 "d2h_bytes_per_step": int(4 * nwin * nc * nf),
-                "note": "MWFJ returns float64 (the reference's dtype): the float32 result is "
-                        "converted on the host inside the timed region"},
+                "note": "MWFJ returns float64 (the reference's dtype): the library copies the "
+                        "float32 result out through pinned staging on several host threads and "
+                        "converts it to float64 on the way, inside the timed region"},
         "roofline": rl,
         "accuracy": {"max_abs_err_vs_fp64_normalised": _err(y32, y64),
                      "nan_positions_equal_fp64": _nan_equal(y32, y64),

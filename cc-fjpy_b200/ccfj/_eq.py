@@ -37,6 +37,7 @@ class EqArgs(ctypes.Structure):
         ("win_delta", ctypes.c_void_p),
         ("out", ctypes.c_void_p),
         ("tau", ctypes.c_float),
+        ("out_f64", ctypes.c_int),
     ]
 
 
@@ -88,7 +89,8 @@ def _win_params(npts, Fs, T1, T2, taper):
             di.astype(np.int32))
 
 
-def _run(u, r, c, f, fstride, itype, func, nwin=0, wins=None, precision=_lib.PREC_FP32):
+def _run(u, r, c, f, fstride, itype, func, nwin=0, wins=None, precision=_lib.PREC_FP32,
+         dtype=np.float32):
     lib = _lib.load()
     u = np.asarray(u)
     nr, nc, nf = len(r), len(c), len(f)
@@ -108,7 +110,10 @@ def _run(u, r, c, f, fstride, itype, func, nwin=0, wins=None, precision=_lib.PRE
     c32 = np.ascontiguousarray(c, dtype=np.float32)
     perm = np.ascontiguousarray(indx, dtype=np.int64)
     nw = max(nwin, 1)
-    out = np.empty((nw, nc, nf) if nwin > 0 else (nc, nf), dtype=np.float32)
+    # float64 (MWFJ's result) is converted by the library while it copies out
+    out = np.empty((nw, nc, nf) if nwin > 0 else (nc, nf), dtype=np.dtype(dtype))
+    if out.dtype not in (np.float32, np.float64):
+        raise ValueError("dtype must be float32 or float64")
     a = EqArgs()
     a.struct_size = ctypes.sizeof(EqArgs)
     a.ntr, a.npts, a.nf, a.nc = nr, npts, nf, nc
@@ -120,6 +125,7 @@ def _run(u, r, c, f, fstride, itype, func, nwin=0, wins=None, precision=_lib.PRE
         n1, n2, dl = wins
         a.win_n1, a.win_n2, a.win_delta = n1.ctypes.data, n2.ctypes.data, dl.ctypes.data
     a.out = out.ctypes.data
+    a.out_f64 = int(out.dtype == np.float64)
     _lib.check(lib.ccfj_fj_earthquake_v1(ctypes.byref(a), None))
     return out
 
@@ -166,5 +172,4 @@ def MWFJ(u, r, c, f, Fs, nwin, winl, winr, taper=0.9, fstride=1, itype=1, func=0
     winr = np.asarray(winr, dtype=np.float64)[:nwin, :nr]
     n1, n2, dl = _win_params(npts, Fs, winl, winr, taper)
     wins = tuple(np.ascontiguousarray(x, dtype=np.int32) for x in (n1, n2, dl))
-    out = _run(u[:nr], r, c, f, fstride, itype, func, nwin=nwin, wins=wins)
-    return out.astype(np.float64)
+    return _run(u[:nr], r, c, f, fstride, itype, func, nwin=nwin, wins=wins, dtype=np.float64)

@@ -70,6 +70,12 @@ class Scratch {
     if (!(cond)) return ::ccfj::set_error(CCFJ_ERR_INVALID, __VA_ARGS__);                    \
   } while (0)
 
+// Copies a result from device memory to host memory `dst` (pageable or
+// pinned) after the work queued on `s`, and waits for it. kind 0: `n`
+// bytes; kind 1: `n` floats stored as doubles. Large copies run through
+// pinned staging buffers on several host threads (host_copy.cu).
+int copy_to_host(void* dst, const void* dsrc, size_t n, int kind, cudaStream_t s);
+
 // Optional event timer around the main transform kernel (ccfj_profile_enable).
 void prof_begin(cudaStream_t s);
 void prof_end(cudaStream_t s);

@@ -565,10 +565,7 @@ int batch_host(const ccfj_batch_args& a, cudaStream_t s) {
   d.perm = dp;
   int st = batch_device(d, total, s);
   if (st != CCFJ_OK) return st;
-  CCFJ_CUDA_TRY(cudaMemcpyAsync(a.out, dout, sizeof(float) * a.nsets * a.nc * a.nf,
-                                cudaMemcpyDeviceToHost, s));
-  CCFJ_CUDA_TRY(cudaStreamSynchronize(s));
-  return CCFJ_OK;
+  return copy_to_host(a.out, dout, sizeof(float) * a.nsets * a.nc * a.nf, 0, s);
 }
 
 }  // namespace

@@ -49,6 +49,9 @@ static int eq_validate(const ccfj_eq_args* a) {
   CCFJ_REQUIRE(a->u_ld >= a->npts, "ccfj_fj_earthquake_v1: u_ld %lld < npts %d", a->u_ld, a->npts);
   CCFJ_REQUIRE(a->u_rows >= a->ntr, "ccfj_fj_earthquake_v1: u_rows %lld < ntr %d", a->u_rows,
                a->ntr);
+  CCFJ_REQUIRE(a->out_f64 == 0 || a->out_f64 == 1, "ccfj_fj_earthquake_v1: out_f64 must be 0 or 1");
+  CCFJ_REQUIRE(!(a->out_f64 && a->device_ptrs),
+               "ccfj_fj_earthquake_v1: out_f64 needs host pointers (device_ptrs = 0)");
   CCFJ_REQUIRE(a->nwin >= 0, "ccfj_fj_earthquake_v1: nwin must be >= 0");
   CCFJ_REQUIRE(a->nwin == 0 || (a->win_n1 && a->win_n2 && a->win_delta),
                "ccfj_fj_earthquake_v1: nwin > 0 needs win_n1/win_n2/win_delta");
@@ -140,6 +143,7 @@ static int eq_host(const ccfj_eq_args& a, cudaStream_t s) {
   Scratch sc(s);
   ccfj_eq_args d = a;
   d.device_ptrs = 1;
+  d.out_f64 = 0;
   const int nw = a.nwin > 0 ? a.nwin : 1;
   const size_t ubytes = sizeof(float) * ((size_t)(a.u_rows - 1) * a.u_ld + a.npts);
   float* du = static_cast<float*>(sc.get(ubytes));
@@ -180,8 +184,10 @@ static int eq_host(const ccfj_eq_args& a, cudaStream_t s) {
   d.out = dout;
   int st = eq_device(d, s, derr);
   if (st != CCFJ_OK) return st;
-  CCFJ_CUDA_TRY(cudaMemcpyAsync(a.out, dout, sizeof(float) * nw * a.nc * a.nf,
-                                cudaMemcpyDeviceToHost, s));
+  const size_t nout = (size_t)nw * a.nc * a.nf;
+  st = a.out_f64 ? copy_to_host(a.out, dout, nout, 1, s)
+                 : copy_to_host(a.out, dout, sizeof(float) * nout, 0, s);
+  if (st != CCFJ_OK) return st;
   bool failed = false;
   st = mw_tc_call_error(derr, s, &failed);
   if (st != CCFJ_OK) return st;

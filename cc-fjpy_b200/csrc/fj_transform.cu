@@ -893,9 +893,7 @@ static int fj_host(const ccfj_fj_args& a, cudaStream_t s) {
   d.out = dout;
   int st = fj_device(d, s);
   if (st != CCFJ_OK) return st;
-  CCFJ_CUDA_TRY(cudaMemcpyAsync(a.out, dout, sizeof(float) * a.nc * a.nf, cudaMemcpyDeviceToHost, s));
-  CCFJ_CUDA_TRY(cudaStreamSynchronize(s));
-  return CCFJ_OK;
+  return copy_to_host(a.out, dout, sizeof(float) * a.nc * a.nf, 0, s);
 }
 
 int fj_entry(const ccfj_fj_args* a, cudaStream_t s) {

@@ -373,15 +373,16 @@ static int run(const ccfj_cc_args& a, cudaStream_t s) {
   }
 
   if (!a.device_ptrs) {
-    if (nout > 0) {
-      if (a.out_layout == 1) {
-        CCFJ_CUDA_TRY(cudaMemcpyAsync(a.out_re, d_re, 2 * plane, cudaMemcpyDeviceToHost, s));
-      } else {
-        CCFJ_CUDA_TRY(cudaMemcpyAsync(a.out_re, d_re, plane, cudaMemcpyDeviceToHost, s));
-        CCFJ_CUDA_TRY(cudaMemcpyAsync(a.out_im, d_im, plane, cudaMemcpyDeviceToHost, s));
-      }
+    int st = CCFJ_OK;
+    if (nout > 0 && a.out_layout == 1) {
+      st = copy_to_host(a.out_re, d_re, 2 * plane, 0, s);
+    } else if (nout > 0) {
+      st = copy_to_host(a.out_re, d_re, plane, 0, s);
+      if (st == CCFJ_OK) st = copy_to_host(a.out_im, d_im, plane, 0, s);
+    } else {
+      CCFJ_CUDA_TRY(cudaStreamSynchronize(s));
     }
-    CCFJ_CUDA_TRY(cudaStreamSynchronize(s));
+    if (st != CCFJ_OK) return st;
   }
   return CCFJ_OK;
 }
@@ -464,11 +465,7 @@ static int cc_fj_noise(const ccfj_cc_args& cc, const ccfj_fj_args& fj, cudaStrea
   if (st != CCFJ_OK) return st;
   st = fj_device(f, s);
   if (st != CCFJ_OK) return st;
-  if (!fj.device_ptrs) {
-    CCFJ_CUDA_TRY(cudaMemcpyAsync(fj.out, f.out, sizeof(float) * fj.nc * fj.nf,
-                                  cudaMemcpyDeviceToHost, s));
-    CCFJ_CUDA_TRY(cudaStreamSynchronize(s));
-  }
+  if (!fj.device_ptrs) return copy_to_host(fj.out, f.out, sizeof(float) * fj.nc * fj.nf, 0, s);
   return CCFJ_OK;
 }
 

@@ -226,6 +226,9 @@ typedef struct ccfj_eq_args {
   const int *win_delta;
   float *out;
   float tau;           /* as ccfj_fj_args.tau                                   */
+  int out_f64;         /* 1: out points to doubles (MWFJ's result type); host
+                          pointers only. The result is converted while it is
+                          copied out. 0: floats                                 */
 } ccfj_eq_args;
 
 CCFJ_API int ccfj_fj_earthquake_v1(const ccfj_eq_args *args, void *stream);

@@ -118,6 +118,24 @@ def test_earthquake_rejects_more_fft_rows_than_a_grid_holds(lib):
     assert "exceed 2^31-1" in lib.ccfj_last_error().decode()
 
 
+@pytest.mark.parametrize("out_f64,device_ptrs,needle", [(2, 0, "out_f64 must be 0 or 1"),
+                                                         (1, 1, "out_f64 needs host pointers")])
+def test_earthquake_double_output_validation(lib, out_f64, device_ptrs, needle):
+    """A double result (MWFJ's type) is converted while the library copies it
+    out, so it exists for host pointers only."""
+    from ccfj import _eq
+    a = _eq.EqArgs()
+    a.struct_size = ctypes.sizeof(a)
+    a.ntr, a.npts, a.nf, a.nc = 4, 64, 8, 4
+    a.itype, a.func, a.fstride, a.nwin = 1, 0, 1, 0
+    a.u_ld, a.u_rows = 64, 4
+    a.out_f64, a.device_ptrs = out_f64, device_ptrs
+    buf = np.zeros(64, dtype=np.float32)
+    a.u = a.r = a.f = a.c = a.out = buf.ctypes.data
+    assert lib.ccfj_fj_earthquake_v1(ctypes.byref(a), None) == 1
+    assert needle in lib.ccfj_last_error().decode()
+
+
 def test_batch_autotuner_needs_device_pointers(lib):
     """ccfj_autotune_batch_v1 validates like the batch entry and times only
     device-resident batches (host-memory calls would time the copies)."""
