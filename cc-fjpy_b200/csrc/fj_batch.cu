@@ -20,6 +20,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "fj_cells.cuh"
 
@@ -515,6 +516,64 @@ int batch_run_device(const ccfj_batch_args& a, long long total, cudaStream_t s) 
   return batch_device(a, total, s);
 }
 
+// ------------------------------------------------- host-memory batches
+// A large batch from host memory is run in groups of consecutive sets, the
+// copy of group g + 1 on a stream of its own while group g computes, so
+// that only the first group's copy is exposed. Group g ends at the first set
+// boundary at or past kGroupEnd[g] of the pairs (the first group is small:
+// its copy is the part that cannot overlap).
+constexpr double kGroupEnd[] = {1.0 / 16, 0.25, 0.5, 0.75, 1.0};
+constexpr size_t kPipelineBytes = (size_t)256 << 20;  // inputs below this: one copy, one pass
+
+struct SetGroup {
+  int b0, b1;                // sets [b0, b1)
+  long long row_lo, row_hi;  // rows of u its pairs read, [row_lo, row_hi]
+};
+
+// Groups of a host batch with one input, or none (one pass) where the
+// input is small, there is one set, or the groups' rows are not disjoint
+// and increasing (a permutation that mixes sets).
+std::vector<SetGroup> plan_groups(const ccfj_batch_args& a, long long total, int nin,
+                                  size_t ubytes) {
+  std::vector<SetGroup> g;
+  if (nin != 1 || a.nsets < 2 || ubytes < kPipelineBytes) return g;
+  const long long* off = a.offsets;
+  int b = 0;
+  for (double end : kGroupEnd) {
+    const long long target = (long long)(end * (double)total);
+    const int b0 = b;
+    while (b < a.nsets && (off[b + 1] <= target || b == b0)) ++b;
+    if (end == 1.0) b = a.nsets;
+    if (b <= b0) continue;
+    long long lo = LLONG_MAX, hi = -1;
+    for (long long i = off[b0]; i < off[b]; ++i) {
+      const long long row = a.perm ? a.perm[i] : i;
+      lo = std::min(lo, row);
+      hi = std::max(hi, row);
+    }
+    if (!g.empty() && lo <= g.back().row_hi) return {};
+    g.push_back({b0, b, lo, hi});
+    if (b == a.nsets) break;
+  }
+  return g.size() > 1 ? g : std::vector<SetGroup>{};
+}
+
+// The copy stream of a pipelined batch and its events; waits for every copy
+// before anything it wrote into is freed (it is declared after the call's
+// Scratch, so it goes first).
+struct CopyLane {
+  cudaStream_t cs = nullptr;
+  std::vector<cudaEvent_t> ev;
+  ~CopyLane() {
+    if (cs) {
+      cudaStreamSynchronize(cs);
+      cudaStreamDestroy(cs);
+    }
+    for (cudaEvent_t e : ev)
+      if (e) cudaEventDestroy(e);
+  }
+};
+
 int batch_host(const ccfj_batch_args& a, cudaStream_t s) {
   const long long* off = a.offsets;
   CCFJ_REQUIRE(off[0] == 0, "ccfj_fj_batch_v1: offsets[0] must be 0");
@@ -538,16 +597,19 @@ int batch_host(const ccfj_batch_args& a, cudaStream_t s) {
   }
   CCFJ_REQUIRE(nin == 1 || (size_t)(hi - lo) <= (size_t)(2 * span + 16),
                "ccfj_fj_batch_v1: host mode needs both inputs in one array (real/imaginary parts)");
+  const size_t ubytes = sizeof(float) * (size_t)(hi - lo);
+  const std::vector<SetGroup> groups = plan_groups(a, total, nin, ubytes);
+  const int ng = (int)groups.size();
   Scratch sc(s);
   float* du = sc.get_n<float>(hi - lo);
-  long long* doff = sc.get_n<long long>(a.nsets + 1);
+  long long* doff = sc.get_n<long long>(a.nsets + 1 + ng);
   float* dr = sc.get_n<float>(total);
   float* df = sc.get_n<float>(a.nf);
   float* dc = sc.get_n<float>(a.nc);
   float* dout = sc.get_n<float>((size_t)a.nsets * a.nc * a.nf);
   long long* dp = a.perm ? sc.get_n<long long>(total) : nullptr;
   if (!du || !doff || !dr || !df || !dc || !dout || (a.perm && !dp)) return CCFJ_ERR_ALLOC;
-  CCFJ_CUDA_TRY(cudaMemcpyAsync(du, lo, sizeof(float) * (hi - lo), cudaMemcpyHostToDevice, s));
+  if (ng == 0) CCFJ_CUDA_TRY(cudaMemcpyAsync(du, lo, ubytes, cudaMemcpyHostToDevice, s));
   CCFJ_CUDA_TRY(cudaMemcpyAsync(doff, off, sizeof(long long) * (a.nsets + 1), cudaMemcpyHostToDevice, s));
   CCFJ_CUDA_TRY(cudaMemcpyAsync(dr, a.r, sizeof(float) * total, cudaMemcpyHostToDevice, s));
   CCFJ_CUDA_TRY(cudaMemcpyAsync(df, a.f, sizeof(float) * a.nf, cudaMemcpyHostToDevice, s));
@@ -563,9 +625,58 @@ int batch_host(const ccfj_batch_args& a, cudaStream_t s) {
   d.c = dc;
   d.out = dout;
   d.perm = dp;
-  int st = batch_device(d, total, s);
+  const size_t out_bytes = sizeof(float) * a.nsets * a.nc * a.nf;
+  if (ng == 0) {
+    const int st = batch_device(d, total, s);
+    if (st != CCFJ_OK) return st;
+    return copy_to_host(a.out, dout, out_bytes, 0, s);
+  }
+
+  // Pipelined: each group's offsets rebased to its first pair (one copy for
+  // all groups, after the whole batch's), its rows of u on the copy stream.
+  std::vector<long long> goff;
+  goff.reserve(a.nsets + ng);
+  for (const SetGroup& g : groups)
+    for (int b = g.b0; b <= g.b1; ++b) goff.push_back(off[b] - off[g.b0]);
+  long long* dgoff = doff + a.nsets + 1;
+  CCFJ_CUDA_TRY(cudaMemcpyAsync(dgoff, goff.data(), sizeof(long long) * goff.size(),
+                                cudaMemcpyHostToDevice, s));
+  // goff may go, and the scratch allocated on s may be used on the copy stream
+  CCFJ_CUDA_TRY(cudaStreamSynchronize(s));
+  CopyLane lane;
+  CCFJ_CUDA_TRY(cudaStreamCreateWithFlags(&lane.cs, cudaStreamNonBlocking));
+  lane.ev.assign(ng, nullptr);
+  for (cudaEvent_t& e : lane.ev) CCFJ_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  auto copy_group = [&](int g) -> int {
+    const long long f0 = groups[g].row_lo * a.u_ld;
+    const long long f1 = groups[g].row_hi * a.u_ld + (long long)(a.u_ncols - 1) * a.u_es + 1;
+    CCFJ_CUDA_TRY(cudaMemcpyAsync(du + f0, lo + f0, sizeof(float) * (f1 - f0),
+                                  cudaMemcpyHostToDevice, lane.cs));
+    CCFJ_CUDA_TRY(cudaEventRecord(lane.ev[g], lane.cs));
+    return CCFJ_OK;
+  };
+  int st = copy_group(0);
   if (st != CCFJ_OK) return st;
-  return copy_to_host(a.out, dout, sizeof(float) * a.nsets * a.nc * a.nf, 0, s);
+  const int variant = batch_variant(a, total);  // the whole batch's choice for every group
+  long long slot = 0;
+  for (int g = 0; g < ng; ++g) {
+    const SetGroup& G = groups[g];
+    ccfj_batch_args dg = d;
+    dg.nsets = G.b1 - G.b0;
+    dg.offsets = dgoff + slot;
+    slot += dg.nsets + 1;
+    dg.total_pairs = off[G.b1] - off[G.b0];
+    dg.r = dr + off[G.b0];
+    dg.perm = dp ? dp + off[G.b0] : nullptr;
+    if (!dp) dg.u[0] = d.u[0] + off[G.b0] * a.u_ld;  // rows are pair indices
+    dg.out = dout + (size_t)G.b0 * a.nc * a.nf;
+    dg.variant = variant;
+    CCFJ_CUDA_TRY(cudaStreamWaitEvent(s, lane.ev[g], 0));
+    st = batch_device(dg, dg.total_pairs, s);
+    if (st != CCFJ_OK) return st;
+    if (g + 1 < ng && (st = copy_group(g + 1)) != CCFJ_OK) return st;
+  }
+  return copy_to_host(a.out, dout, out_bytes, 0, s);
 }
 
 }  // namespace

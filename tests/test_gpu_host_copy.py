@@ -4,9 +4,10 @@ Results of 16 MiB and more go to pageable host memory through pinned
 staging buffers on several host threads; MWFJ's float64 result is converted
 on the way. Checked here: the staged copy equals the device result read by
 torch bit for bit, MWFJ's float64 result is exactly its float32 result
-widened (staged and unstaged sizes), and two calls that overlap on the host
+widened (staged and unstaged sizes), two calls that overlap on the host
 (one takes the staging buffers, the other the plain route) both come back
-right.
+right, and a batch of 256 MB or more of host spectra, run in groups of sets
+with the copies overlapping the transforms, equals one device-resident pass.
 """
 import ctypes
 import threading
@@ -29,17 +30,10 @@ def _noise_batch(nsets=8, nf=600, nc=1000, seed=21):
     return ufs, rs, c, f
 
 
-def test_staged_copy_equals_device_result(lib):
-    """19.2 MB of batch output: the host-memory call (staged copy) against the
-    device-pointer call read back by torch."""
+def _device_batch(lib, ufs, rs, c, f):
+    """The batch with every array on the device (one pass), read back by torch."""
     import torch
-    import ccfj
     from ccfj import _batch, _lib
-    ufs, rs, c, f = _noise_batch()
-    with warnings.catch_warnings():
-        warnings.simplefilter("ignore")
-        host = np.stack(ccfj.fj_noise_batch(ufs, rs, c, f))
-    assert host.nbytes >= 16 << 20
     off = np.concatenate([[0], np.cumsum([len(r) for r in rs])]).astype(np.int64)
     perm = np.concatenate([off[b] + np.argsort(r) for b, r in enumerate(rs)]).astype(np.int64)
     rsorted = np.concatenate([np.sort(r) for r in rs]).astype(np.float32)
@@ -47,7 +41,7 @@ def test_staged_copy_equals_device_result(lib):
     T = {k: torch.from_numpy(np.ascontiguousarray(v)).cuda() for k, v in dict(
         u=U.view(np.float32), off=off, perm=perm, r=rsorted, f=f.astype(np.float32),
         c=c.astype(np.float32)).items()}
-    out = torch.empty(host.shape, device="cuda")
+    out = torch.empty((len(rs), len(c), len(f)), device="cuda")
     a = _batch.BatchArgs()
     a.struct_size = ctypes.sizeof(a)
     a.nsets, a.nf, a.nc = len(rs), len(f), len(c)
@@ -60,7 +54,39 @@ def test_staged_copy_equals_device_result(lib):
     torch.cuda.synchronize()
     _lib.check(lib.ccfj_fj_batch_v1(ctypes.byref(a), None))
     torch.cuda.synchronize()
-    assert np.array_equal(out.cpu().numpy(), host, equal_nan=True)
+    return out.cpu().numpy()
+
+
+def test_staged_copy_equals_device_result(lib):
+    """19.2 MB of batch output: the host-memory call (staged copy) against the
+    device-pointer call read back by torch."""
+    import ccfj
+    ufs, rs, c, f = _noise_batch()
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        host = np.stack(ccfj.fj_noise_batch(ufs, rs, c, f))
+    assert host.nbytes >= 16 << 20
+    assert np.array_equal(_device_batch(lib, ufs, rs, c, f), host, equal_nan=True)
+
+
+def test_pipelined_host_batch_equals_device_batch(lib):
+    """328 MB of complex64 spectra from host memory run in groups of sets,
+    the next group's copy overlapping the current group's transform; equal
+    bit for bit to one device-resident pass over all sets."""
+    import ccfj
+    rng = np.random.default_rng(23)
+    nf, nc = 1024, 16
+    f = np.linspace(0.01, 1.0, nf)
+    c = np.linspace(1500.0, 4500.0, nc)
+    counts = rng.integers(1000, 4000, 16)
+    counts[-1] += 40000 - counts.sum() if counts.sum() < 40000 else 0
+    rs = [rng.uniform(1e3, 4e4, n) for n in counts]
+    ufs = [cases.noise_spectra(rng, r, f) for r in rs]
+    assert sum(u.nbytes for u in ufs) >= 256 << 20
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        host = np.stack(ccfj.fj_noise_batch(ufs, rs, c, f))
+    assert np.array_equal(_device_batch(lib, ufs, rs, c, f), host, equal_nan=True)
 
 
 @pytest.mark.parametrize("nwin,nc", [(16, 600), (8, 40)])
@@ -88,8 +114,8 @@ def test_mwfj_double_result_is_the_float_result_widened(nwin, nc):
 
 
 def test_overlapping_host_calls():
-    """Two threads copy large results out at the same time: one holds the
-    staging buffers, the other takes the plain route; both are right."""
+    """Four threads copy large results out at the same time: one holds the
+    staging buffers, the others take the plain route; all are right."""
     import ccfj
     ufs, rs, c, f = _noise_batch(seed=22)
     with warnings.catch_warnings():
