@@ -52,9 +52,11 @@ class Scratch {
 #define CCFJ_CUDA_TRY(expr)                                                                  \
   do {                                                                                       \
     cudaError_t e__ = (expr);                                                                \
-    if (e__ != cudaSuccess)                                                                  \
+    if (e__ != cudaSuccess) {                                                                \
+      cudaGetLastError(); /* a non-sticky error must not fail a later launch check */       \
       return ::ccfj::set_error(CCFJ_ERR_CUDA, "%s failed: %s (%s:%d)", #expr,                \
                                cudaGetErrorString(e__), __FILE__, __LINE__);                 \
+    }                                                                                        \
   } while (0)
 
 #define CCFJ_LAUNCH_CHECK(name)                                                              \

@@ -602,7 +602,8 @@ int batch_host(const ccfj_batch_args& a, cudaStream_t s) {
   const int ng = (int)groups.size();
   Scratch sc(s);
   float* du = sc.get_n<float>(hi - lo);
-  long long* doff = sc.get_n<long long>(a.nsets + 1 + ng);
+  // the batch's offsets, then (pipelined) each group's rebased offsets
+  long long* doff = sc.get_n<long long>(a.nsets + 1 + (ng > 0 ? a.nsets + ng : 0));
   float* dr = sc.get_n<float>(total);
   float* df = sc.get_n<float>(a.nf);
   float* dc = sc.get_n<float>(a.nc);
