@@ -201,6 +201,32 @@ __device__ __forceinline__ float2 twiddle_full(const float2* __restrict__ tw, in
   return t < h ? w : make_float2(-w.x, -w.y);
 }
 
+// w[r] = e^{-2 pi i r t / M} for r < R (r t < M): the table entries of t,
+// 2t, 4t and 8t, the other powers as products of those (at most three
+// products deep, a few ulp). The twiddle indices of a warp's lanes are far
+// apart in the table, so each table read costs one L1 wavefront per lane
+// group; four reads per butterfly instead of R - 1.
+template <int R>
+__device__ __forceinline__ void twiddle_powers(const float2* __restrict__ tw, int t, int M,
+                                               float2 (&w)[R]) {
+  w[0] = make_float2(1.0f, 0.0f);
+  w[1] = twiddle_full(tw, t, M);
+  if (R >= 4) {
+    w[2 % R] = twiddle_full(tw, 2 * t, M);
+    w[3 % R] = cmul(w[1], w[2 % R]);
+  }
+  if (R >= 8) {
+    w[4 % R] = twiddle_full(tw, 4 * t, M);
+#pragma unroll
+    for (int r = 5; r < 8; ++r) w[r % R] = cmul(w[4 % R], w[(r - 4) % R]);
+  }
+  if (R >= 16) {
+    w[8 % R] = twiddle_full(tw, 8 * t, M);
+#pragma unroll
+    for (int r = 9; r < 16; ++r) w[r % R] = cmul(w[8 % R], w[(r - 8) % R]);
+  }
+}
+
 // One Stockham pass of radix R over the 16 registers of thread tid (16/R
 // butterflies j = tid + g P), writing the outputs to shared memory.
 template <int R>
@@ -212,9 +238,10 @@ __device__ __forceinline__ void stockham_pass(float2 (&v)[16], float2* sz, int M
     const int k = j % Ns;
     float2* u = v + g * R;
     if (Ns > 1) {
-      const int step = k * (M / (Ns * R));
+      float2 w[R];
+      twiddle_powers<R>(tw, k * (M / (Ns * R)), M, w);
 #pragma unroll
-      for (int r = 1; r < R; ++r) u[r] = cmul(u[r], twiddle_full(tw, r * step, M));
+      for (int r = 1; r < R; ++r) u[r] = cmul(u[r], w[r]);
     }
     dft_pow2<R>(u);
     const int o = (j / Ns) * Ns * R + k;
