@@ -98,8 +98,8 @@ static int eq_device(const ccfj_eq_args& a, cudaStream_t s, unsigned int* call_e
     // tensor cores when the window dimension makes the contraction dense
     const bool tc_ok = a.itype == 1 && a.func == 0 && a.ntr >= 2 && a.nwin <= 128;
     const int path = g_mwfj_path.load(std::memory_order_relaxed);
-    const bool use_tc = tc_ok && (path == 2 || (path == 0 && a.nwin >= 8));
-    if (use_tc) return mwfj_tensor(a, spec, s, sc, call_err);
+    const bool use_tc = tc_ok && (path >= 2 || (path == 0 && a.nwin >= 8));
+    if (use_tc) return mwfj_tensor(a, spec, s, sc, call_err, path != 3);
     return mwfj_cuda_core(a, spec, s, sc);
   }
 
@@ -201,8 +201,8 @@ std::atomic<int> g_mwfj_path{0};
 }  // namespace ccfj
 
 CCFJ_API int ccfj_set_mwfj_path(int path) {
-  if (path < 0 || path > 2)
-    return ccfj::set_error(CCFJ_ERR_INVALID, "ccfj_set_mwfj_path: path must be 0, 1 or 2");
+  if (path < 0 || path > 3)
+    return ccfj::set_error(CCFJ_ERR_INVALID, "ccfj_set_mwfj_path: path must be 0, 1, 2 or 3");
   ccfj::g_mwfj_path.store(path, std::memory_order_relaxed);
   return CCFJ_OK;
 }

@@ -36,8 +36,10 @@ int mwfj_cuda_core(const ccfj_eq_args& a, const float2* spec, cudaStream_t s, Sc
 // The same contraction on the tensor cores (tcgen05, scaled FP16x3): itype 1,
 // func 0, 2 <= nr, nwin <= 128.
 // call_err: a device word for this call's timeout flag (NULL: taken from sc).
+// paired: the A-operand generator with paired FP32 arithmetic (else one
+// interval at a time; the results agree to rounding).
 int mwfj_tensor(const ccfj_eq_args& a, const float2* spec, cudaStream_t s, Scratch& sc,
-                unsigned int* call_err);
+                unsigned int* call_err, bool paired = true);
 // Waits for `s` and reads one call's timeout flag.
 int mw_tc_call_error(const unsigned int* err, cudaStream_t s, bool* failed);
 // Waits for `s`, reads the process-wide timeout flag of the tensor kernel

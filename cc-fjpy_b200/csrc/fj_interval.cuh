@@ -78,4 +78,52 @@ FJ_HD void interval_moments(const Station<T>& a, const Station<T>& b, T dx, bool
   }
 }
 
+#if defined(FJS_HAVE_PAIRED)
+// Two stations (or two intervals) per paired FP32 instruction: the lanes
+// carry independent values, each computed with make_station's and
+// interval_moments' operations (a - b as fma(-1, b, a), a single rounding
+// like the subtraction).
+struct Station2 {
+  float2 h, hp, hpp, xz1, b;
+};
+
+__device__ __forceinline__ float2 psub(float2 a, float2 b) { return pfma(psplat(-1.0f), b, a); }
+
+__device__ __forceinline__ Station2 make_station_pair(float2 x, const ZB2& z, float2 b) {
+  Station2 s;
+  s.h = pmul(x, z.z0);
+  s.xz1 = pmul(x, z.z1);
+  s.hp = psub(z.z0, s.xz1);
+  s.hpp = pmul(psplat(-1.0f), padd(z.z1, s.h));
+  s.b = b;
+  return s;
+}
+
+__device__ __forceinline__ Station<float> station_lane(const Station2& s, int lane) {
+  return lane == 0 ? Station<float>{s.h.x, s.hp.x, s.hpp.x, s.xz1.x, s.b.x}
+                   : Station<float>{s.h.y, s.hp.y, s.hpp.y, s.xz1.y, s.b.y};
+}
+
+// interval_moments of two intervals (a.x -> b.x, a.y -> b.y) that take the
+// same rule.
+__device__ __forceinline__ void interval_moments_pair(const Station2& a, const Station2& b,
+                                                      float2 dx, bool closed, float2& I0,
+                                                      float2& I1) {
+  if (closed) {
+    I0 = psub(b.xz1, a.xz1);
+    I1 = pfma(dx, b.xz1, psub(psub(b.h, a.h), psub(b.b, a.b)));
+  } else {
+    const float2 c1 = pmul(psplat(0.5f), dx);
+    const float2 d2 = pmul(dx, dx);
+    const float2 c2 = pmul(psplat(0.1f), d2);
+    const float2 c3 = pmul(pmul(d2, dx), psplat((float)(1.0 / 120.0)));
+    I0 = pfma(c1, padd(a.h, b.h), pfma(c2, psub(a.hp, b.hp), pmul(c3, padd(a.hpp, b.hpp))));
+    const float2 g0 = pmul(dx, b.h);
+    const float2 g0p = pfma(dx, b.hp, b.h);
+    const float2 g0pp = pfma(dx, b.hpp, pmul(psplat(2.0f), b.hp));
+    I1 = pfma(c1, g0, pfma(c2, psub(a.h, g0p), pmul(c3, pfma(psplat(2.0f), a.hp, g0pp))));
+  }
+}
+#endif
+
 }  // namespace fjs

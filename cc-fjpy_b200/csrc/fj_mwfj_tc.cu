@@ -216,6 +216,11 @@ __device__ __forceinline__ int tile_off(int row, int k, int rows) {
   return slice * rows * 32 + (row >> 3) * 256 + (kk >> 3) * 128 + (row & 7) * 16 + (kk & 7) * 2;
 }
 
+// PAIRED: where both stations of two consecutive intervals have x >= 8, the
+// two stations are evaluated, and the two intervals' moments formed, with
+// paired FP32 instructions (one lane per station); elsewhere, and without
+// PAIRED, one interval at a time.
+template <bool PAIRED>
 __global__ void __launch_bounds__(tc::kThreads, 2) fj_mw_tc_kernel(MwTcDev a) {
   extern __shared__ __align__(1024) unsigned char smem[];
   const int tid = threadIdx.x;
@@ -297,33 +302,86 @@ __global__ void __launch_bounds__(tc::kThreads, 2) fj_mw_tc_kernel(MwTcDev a) {
     // A of this chunk: I0 and I1/k of intervals 1 + 16 kc + j
     unsigned char* aHi = sA + s * TcSmem::kABytesStage + mh * (2 * tc::kSlices * tc::kSliceBytes128);
     unsigned char* aLo = aHi + tc::kSlices * tc::kSliceBytes128;
+    // interval i (stations i - 1, i): I0 and I1 / (k s), scaled
+    auto one_interval = [&](int i, float& I0, float& I1k) {
+      I0 = 0.f;
+      I1k = 0.f;
+      if (i < a.nr) {
+        const float r = __ldg(a.rs + i);
+        const float dr = dr_next;
+        const float inv_s = dn.y;  // 1 / max(dr, 0.1)
+        dn = __ldg(a.dinv + i + 1);
+        dr_next = dn.x;
+        const float x = cell.k * r;
+        const float dx = cell.k * dr;
+        const bool lc = ln;
+        ln = closed_form<float, false>(cell.k * dr_next, x, tau);
+        cell.eval<true, false, true>(r, x, lc || ln, Jz, Yz);
+        const Station<float> st = fjs::make_station(x, Jz);
+        float I1;
+        fjs::interval_moments<float>(sp, st, dx, lc, I0, I1);
+        sp = st;
+        I0 *= c0s;
+        I1k = I1 * c1s * inv_s;
+      }
+    };
 #pragma unroll 1
     for (int j4 = 0; j4 < tc::kChunkI; j4 += 4) {
       __half2 hi[4], lo[4];
 #pragma unroll
-      for (int jj = 0; jj < 4; ++jj) {
+      for (int jj = 0; jj < 4; jj += 2) {
         const int i = 1 + kc * tc::kChunkI + j4 + jj;
-        float I0 = 0.f, I1k = 0.f;
-        if (i < a.nr) {
-          const float r = __ldg(a.rs + i);
-          const float dr = dr_next;
-          const float inv_s = dn.y;  // 1 / max(dr, 0.1)
-          dn = __ldg(a.dinv + i + 1);
-          dr_next = dn.x;
-          const float x = cell.k * r;
-          const float dx = cell.k * dr;
-          const bool lc = ln;
-          ln = closed_form<float, false>(cell.k * dr_next, x, tau);
-          cell.eval<true, false, true>(r, x, lc || ln, Jz, Yz);
-          const Station<float> st = fjs::make_station(x, Jz);
-          float I1;
-          fjs::interval_moments<float>(sp, st, dx, lc, I0, I1);
-          sp = st;
-          xp = x;
-          I0 *= c0s;
-          I1k = I1 * c1s * inv_s;
+        float2 I0 = make_float2(0.f, 0.f), I1k = make_float2(0.f, 0.f);
+        bool done = false;
+#if defined(FJS_HAVE_PAIRED)
+        if (PAIRED && i + 1 < a.nr) {
+          const float2 rr = make_float2(__ldg(a.rs + i), __ldg(a.rs + i + 1));
+          const float2 x = fjs::pmul(fjs::psplat(cell.k), rr);
+          if (x.x >= 8.0f && x.y >= 8.0f) {
+            // intervals i and i + 1; the state then stands after i + 1
+            const float2 dn1 = __ldg(a.dinv + i + 1), dn2 = __ldg(a.dinv + i + 2);
+            const float2 dx = fjs::pmul(fjs::psplat(cell.k), make_float2(dr_next, dn1.x));
+            const float2 inv_s = make_float2(dn.y, dn1.y);
+            const bool lc0 = ln;
+            const bool lc1 = closed_form<float, false>(cell.k * dn1.x, x.x, tau);
+            ln = closed_form<float, false>(cell.k * dn2.x, x.y, tau);
+            dn = dn2;
+            dr_next = dn2.x;
+            float2 p_hi, p_lo;
+            p_hi.x = cell.q_hi * rr.x;
+            p_lo.x = fmaf(cell.q_lo, rr.x, fmaf(cell.q_hi, rr.x, -p_hi.x));
+            p_hi.y = cell.q_hi * rr.y;
+            p_lo.y = fmaf(cell.q_lo, rr.y, fmaf(cell.q_hi, rr.y, -p_hi.y));
+            fjs::ZB2 J2;
+            float2 b2 = make_float2(0.f, 0.f);
+            fjs::eval_large_pair_stations_j(x, p_hi, p_lo, lc0 || lc1 || ln, J2, b2);
+            const fjs::Station2 st = fjs::make_station_pair(x, J2, b2);
+            if (lc0 == lc1) {
+              const fjs::Station2 sa{make_float2(sp.h, st.h.x), make_float2(sp.hp, st.hp.x),
+                                     make_float2(sp.hpp, st.hpp.x), make_float2(sp.xz1, st.xz1.x),
+                                     make_float2(sp.b, st.b.x)};
+              float2 I1;
+              fjs::interval_moments_pair(sa, st, dx, lc0, I0, I1);
+              I1k = fjs::pmul(fjs::pmul(I1, fjs::psplat(c1s)), inv_s);
+            } else {
+              const Station<float> s0 = fjs::station_lane(st, 0);
+              float I1a, I1b;
+              fjs::interval_moments<float>(sp, s0, dx.x, lc0, I0.x, I1a);
+              fjs::interval_moments<float>(s0, fjs::station_lane(st, 1), dx.y, lc1, I0.y, I1b);
+              I1k = fjs::pmul(fjs::pmul(make_float2(I1a, I1b), fjs::psplat(c1s)), inv_s);
+            }
+            I0 = fjs::pmul(I0, fjs::psplat(c0s));
+            sp = fjs::station_lane(st, 1);
+            done = true;
+          }
         }
-        tc::split_f16x2(I0, I1k, hi[jj], lo[jj]);
+#endif
+        if (!done) {
+          one_interval(i, I0.x, I1k.x);
+          one_interval(i + 1, I0.y, I1k.y);
+        }
+        tc::split_f16x2(I0.x, I1k.x, hi[jj], lo[jj]);
+        tc::split_f16x2(I0.y, I1k.y, hi[jj + 1], lo[jj + 1]);
       }
       const int off = tile_off(row, 2 * j4, 128);
       *reinterpret_cast<uint4*>(aHi + off) = *reinterpret_cast<const uint4*>(hi);
@@ -552,7 +610,7 @@ __global__ void mw_tc_bscale_kernel(const float2* __restrict__ spec, int ntr, in
 __device__ unsigned int g_mw_tc_error = 0;
 
 int mwfj_tensor(const ccfj_eq_args& a, const float2* spec, cudaStream_t s, Scratch& sc,
-                unsigned int* call_err) {
+                unsigned int* call_err, bool paired) {
   const int nr = a.ntr, nf = a.nf, nwin = a.nwin;
   CCFJ_REQUIRE(nr >= 2 && nwin >= 1, "MWFJ tensor path: needs nr >= 2 and nwin >= 1");
   int N = 2 * nwin;
@@ -617,9 +675,10 @@ int mwfj_tensor(const ccfj_eq_args& a, const float2* spec, cudaStream_t s, Scrat
   d.wait_cycles = tc::kWaitCycles;
   d.self_test_no_copy = 0;
   const int smem = TcSmem::total(N);
-  CCFJ_CUDA_TRY(cudaFuncSetAttribute(fj_mw_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  auto* kern = paired ? fj_mw_tc_kernel<true> : fj_mw_tc_kernel<false>;
+  CCFJ_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
   prof_begin(s);
-  fj_mw_tc_kernel<<<dim3(div_up(a.nc, tc::kThreads), nf), tc::kThreads, smem, s>>>(d);
+  kern<<<dim3(div_up(a.nc, tc::kThreads), nf), tc::kThreads, smem, s>>>(d);
   prof_end(s);
   count_launch();
   CCFJ_LAUNCH_CHECK("fj_mw_tc_kernel");
@@ -679,8 +738,9 @@ int mw_tc_self_test(cudaStream_t s, int* status) {
   d.wait_cycles = 2000000;  // ~1 ms
   d.self_test_no_copy = 1;
   const int smem = TcSmem::total(N);
-  CCFJ_CUDA_TRY(cudaFuncSetAttribute(fj_mw_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  fj_mw_tc_kernel<<<1, tc::kThreads, smem, s>>>(d);
+  CCFJ_CUDA_TRY(cudaFuncSetAttribute(fj_mw_tc_kernel<true>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  fj_mw_tc_kernel<true><<<1, tc::kThreads, smem, s>>>(d);
   count_launch();
   CCFJ_LAUNCH_CHECK("fj_mw_tc_kernel (self-test)");
   bool failed = false;

@@ -509,6 +509,41 @@ __device__ __forceinline__ void eval_large_scaled_pair_j(const PairPhase& ph, fl
   J.z0 = pfma(P0, cs, pmul(nQ0, sn));  // fma(P0, cs, -Q0 sn)
   J.z1 = pfma(P1, sn, pmul(Q1, cs));   // fma(P1, sn, Q1 cs)
 }
+
+// eval_station_f32<true, false, true> at two stations of one cell, x >= 8
+// in both (lanes are stations): J0, J1 (times the amplitude) and, with
+// need_b, B of both lanes. p_hi / p_lo: each lane's phase x / (2 pi) in
+// cycles, formed by the caller with the scalar code.
+__device__ __forceinline__ void eval_large_pair_stations_j(float2 x, float2 p_hi, float2 p_lo,
+                                                           bool need_b, ZB2& J, float2& B) {
+  float2 sn, cs;
+  sincos_cycles_f32(chi_cycles_f32(p_hi.x, p_lo.x), sn.x, cs.x);
+  sincos_cycles_f32(chi_cycles_f32(p_hi.y, p_lo.y), sn.y, cs.y);
+  const float2 rs = make_float2(rsqrt_fast(x.x), rsqrt_fast(x.y));
+  const float2 M = pmul(psplat(kSqrt2OverPiF), rs);
+  const float2 s = pmul(psplat(8.0f), pmul(rs, rs));
+  const float2 z = pmul(s, s);
+  constexpr float cp0[] = FJC_F32_L_P0;
+  constexpr float cq0[] = FJC_F32_L_Q0;
+  constexpr float cp1[] = FJC_F32_L_P1;
+  constexpr float cq1[] = FJC_F32_L_Q1;
+  const float2 P0 = phorner(cp0, z);
+  const float2 nQ0 = pmul(phorner_neg(cq0, z), s);  // -Q0
+  const float2 P1 = phorner(cp1, z);
+  const float2 Q1 = pmul(phorner(cq1, z), s);
+  const float2 y0 = pfma(P0, cs, pmul(nQ0, sn));
+  const float2 y1 = pfma(P1, sn, pmul(Q1, cs));
+  if (need_b) {
+    // B_J = 1 + M (y1 rho0 - y0 rho1)
+    constexpr float cr0[] = FJC_F32_L_RHO0;
+    constexpr float cr1[] = FJC_F32_L_RHO1;
+    const float2 rho0 = phorner(cr0, z);
+    const float2 nrho1 = pmul(phorner_neg(cr1, z), s);  // -rho1
+    B = pfma(M, pfma(y1, rho0, pmul(y0, nrho1)), psplat(1.0f));
+  }
+  J.z0 = pmul(y0, M);
+  J.z1 = pmul(y1, M);
+}
 #endif
 #endif
 

@@ -236,7 +236,9 @@ CCFJ_API int ccfj_fj_earthquake_v1(const ccfj_eq_args *args, void *stream);
  * FP16x3 (hi/lo fp16 operands with exact power-of-two scales) with FP32
  * accumulation, for itype 1, func 0 and 8 <= nwin <= 128;
  * CUDA-core FMAs otherwise), 1 = always CUDA cores, 2 = tensor cores
- * wherever supported. */
+ * wherever supported, 3 = as 2 with the A operand generated one interval at
+ * a time (no paired FP32 arithmetic; for checks, the results agree with 2
+ * to rounding). */
 CCFJ_API int ccfj_set_mwfj_path(int path);
 /* Waits for `stream` and reports CCFJ_ERR_TIMEOUT if a bounded device-side
  * wait of a tensor-core kernel ran out, in any call on this device, since

@@ -53,6 +53,20 @@ def test_tensor_path_matches_cuda_core_and_oracle(ntr, nwin, nc):
         assert O.rel_error(y_tc[w], O._normalize(y64)) <= TOL
 
 
+@pytest.mark.parametrize("ntr,nwin,nc", [(70, 64, 300), (41, 8, 257)])
+def test_paired_generator_agrees_with_one_interval_at_a_time(ntr, nwin, nc):
+    """The A operand formed with paired FP32 instructions (two stations per
+    instruction where both have x >= 8; an odd pair count leaves a last
+    interval alone) against the one-interval-at-a-time generator (path 3):
+    the same arithmetic up to rounding."""
+    case = _case(91 + ntr, ntr, nwin, nc=nc)
+    y2 = _run(2, case)
+    y3 = _run(3, case)
+    assert np.array_equal(np.isnan(y2), np.isnan(y3))
+    for w in range(nwin):
+        assert O.rel_error(y2[w], y3[w]) <= 1e-5
+
+
 def test_tensor_path_f0_column_is_nan():
     case = _case(77, 20, 16)
     y = _run(2, case)
