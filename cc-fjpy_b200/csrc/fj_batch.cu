@@ -176,9 +176,17 @@ __global__ void batch_normalize_kernel(float* __restrict__ out, int nc, int nf) 
   __shared__ float colmax[32];
   float* o = out + (long long)blockIdx.y * nc * nf;
   const int fi = blockIdx.x * 32 + threadIdx.x;
-  float m = -INFINITY;
-  if (fi < nf)
-    for (int c = threadIdx.y; c < nc; c += blockDim.y) m = fmaxf(m, fabsf(o[(long long)c * nf + fi]));
+  // two running maxima and eight loads in flight per thread (the maximum
+  // does not depend on the order)
+  float m = -INFINITY, m2 = -INFINITY;
+  if (fi < nf) {
+#pragma unroll 8
+    for (int c = threadIdx.y; c < nc; c += 2 * blockDim.y) {
+      m = fmaxf(m, fabsf(o[(long long)c * nf + fi]));
+      if (c + (int)blockDim.y < nc) m2 = fmaxf(m2, fabsf(o[(long long)(c + blockDim.y) * nf + fi]));
+    }
+  }
+  m = fmaxf(m, m2);
   red[threadIdx.y][threadIdx.x] = m;
   __syncthreads();
   if (threadIdx.y == 0) {
@@ -191,6 +199,7 @@ __global__ void batch_normalize_kernel(float* __restrict__ out, int nc, int nf) 
   __syncthreads();
   if (fi < nf) {
     const float dv = colmax[threadIdx.x];
+#pragma unroll 8
     for (int c = threadIdx.y; c < nc; c += blockDim.y) {
       const long long k = (long long)c * nf + fi;
       o[k] = o[k] / dv;
