@@ -141,13 +141,33 @@ CC_HD void bf_load(const Cpx* src, int M, int t, Cpx* v) {
   for (int r = 0; r < R; ++r) v[r] = src[t + r * stride];
 }
 
+// w[r] = tw[r step] for 0 < r < R: the table entries of step, 2 step and
+// (radix 8) 4 step, the other powers as products of those (one or two
+// products deep). The twiddle indices of neighbouring butterflies lie far
+// apart in the table, so fewer reads mean fewer cache wavefronts.
+template <int R>
+CC_HD void twiddle_powers(const Cpx* tw, int step, Cpx* w) {
+  w[1] = tw[step];
+  if (R >= 3) w[2 % R] = tw[2 * step];
+  if (R >= 4) w[3 % R] = cmul(w[1], w[2 % R]);
+  if (R == 5) w[4 % R] = cmul(w[2 % R], w[2 % R]);
+  if (R == 8) {
+    w[4 % R] = tw[4 * step];
+    w[5 % R] = cmul(w[4 % R], w[1]);
+    w[6 % R] = cmul(w[4 % R], w[2 % R]);
+    w[7 % R] = cmul(w[4 % R], w[3 % R]);
+  }
+}
+
 template <int R>
 CC_HD void bf_finish(Cpx* dst, int M, int Ns, const Cpx* tw, int t, Cpx* v) {
   const int jn = t % Ns;
   if (jn != 0) {
     const int step = (M / (Ns * R)) * jn;
+    Cpx w[R];
+    twiddle_powers<R>(tw, step, w);
 #pragma unroll
-    for (int r = 1; r < R; ++r) v[r] = cmul(v[r], tw[r * step]);
+    for (int r = 1; r < R; ++r) v[r] = cmul(v[r], w[r]);
   }
   dft<R>(v);
   const int base = (t / Ns) * Ns * R + jn;
