@@ -520,12 +520,14 @@ __device__ __forceinline__ Acc2<T> explicit_interval(const Cell<T>& cell, bool e
 }
 
 // Minimum resident 256-thread CTAs per SM of the kernels built on
-// fj_cells. FP32: at most 64 registers, four CTAs (more warps to hide the
-// special functions' latency); the single-set and the batch kernels share
+// fj_cells. FP32: three CTAs, at most 85 registers. Two velocities per
+// thread (the paired x >= 8 step) then fit without spilling; under four
+// CTAs (64 registers) they spilled, and the large-array transform measured
+// 5% slower, the small one 6%. The single-set and the batch kernels share
 // the bound, so they compile the cell loop alike and agree bit for bit.
 // FP64 cells hold twice the registers: a cap would only make them spill.
 #ifndef CCFJ_FJ_MIN_BLOCKS
-#define CCFJ_FJ_MIN_BLOCKS 4
+#define CCFJ_FJ_MIN_BLOCKS 3
 #endif
 template <typename T>
 constexpr int fj_min_blocks() { return sizeof(T) == 4 ? CCFJ_FJ_MIN_BLOCKS : 1; }
