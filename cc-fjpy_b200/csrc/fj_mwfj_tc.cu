@@ -24,12 +24,10 @@
 // frequency, all windows (N = 2 nwin padded to a multiple of 16, <= 256).
 // Per chunk of 16 intervals (K = 32): every thread writes its 32 A values
 // (hi and lo) into shared memory in the K-major, no-swizzle canonical
-// layout; one thread waits for the chunk's B (a 1-D bulk copy, issued when
-// its stage is released, while the A operand is generated), issues 12
-// tcgen05.mma and commits them to an mbarrier that releases the stage; the
-// other threads go on to the next chunk. Two stages, two CTA barriers per
-// chunk. All waits are bounded; a wait that runs out sets an error flag,
-// drains what is in flight and returns.
+// layout; one thread waits for the chunk's B (a 1-D bulk copy, issued two
+// chunks ahead), issues 12 tcgen05.mma and commits them to an mbarrier that
+// releases the stage. Two stages. All waits are bounded; a wait that runs
+// out sets an error flag, drains what is in flight and returns.
 #include <cuda_fp16.h>
 #include <stdint.h>
 
@@ -234,10 +232,12 @@ __global__ void __launch_bounds__(tc::kThreads, 2) fj_mw_tc_kernel(MwTcDev a) {
   const int bstage = TcSmem::b_bytes_stage(a.N);
   uint64_t* bar = reinterpret_cast<uint64_t*>(sB + 2 * bstage);  // [0,1] B full, [2,3] MMA done
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 4);
+  __shared__ int abort_flag;
 
   if (tid == 0) {
     for (int j = 0; j < 4; ++j) tc::mbar_init(bar + j, 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    abort_flag = 0;
   }
   if (tid < 32) {  // warp 0 owns the tensor-memory allocation
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
@@ -284,22 +284,15 @@ __global__ void __launch_bounds__(tc::kThreads, 2) fj_mw_tc_kernel(MwTcDev a) {
   int issued_b = a.self_test_no_copy ? 0 : (a.nchunks < 2 ? a.nchunks : 2);  // thread 0's count
   int committed = 0;                             // MMA groups committed (thread 0's count)
 
-  // Every abort decision is the value of a barrier that reduces the
-  // threads' predicates (__syncthreads_or), so all threads take it
-  // together. Two barriers per chunk: the stage's release (from chunk 2 on)
-  // and the A operand's completion; thread 0's B wait of a chunk is judged
-  // at the next chunk's completion barrier (or after the loop).
-  bool aborted = false;  // the same in every thread
-  bool t0_fail = false;  // thread 0: a chunk's B copy did not arrive in time
+  // Every abort decision is taken on abort_flag right after a barrier, so
+  // all threads leave the loop together.
   for (int kc = 0; kc < a.nchunks; ++kc) {
     const int s = kc & 1;
     if (kc >= 2) {
       // the MMAs of chunk kc - 2 released this stage
-      const bool ok = tc::mbar_wait(bar + 2 + s, ((kc >> 1) - 1) & 1, a.wait_cycles);
-      if (__syncthreads_or(!ok)) {
-        aborted = true;
-        break;
-      }
+      if (!tc::mbar_wait(bar + 2 + s, ((kc >> 1) - 1) & 1, a.wait_cycles)) atomicOr(&abort_flag, 1);
+      __syncthreads();
+      if (abort_flag) break;
       if (tid == 0 && !a.self_test_no_copy) {
         tc::mbar_expect_tx(bar + s, bstage);
         tc::bulk_g2s(sB + s * bstage, bsrc + (long long)kc * (bstage / 16), bstage, bar + s);
@@ -396,14 +389,11 @@ __global__ void __launch_bounds__(tc::kThreads, 2) fj_mw_tc_kernel(MwTcDev a) {
     }
     tc::fence_async_smem();
     tc::tc_fence_before();
-    if (__syncthreads_or(t0_fail)) {
-      aborted = true;
-      break;
-    }
+    __syncthreads();
     if (tid == 0) {
       tc::tc_fence_after();
       if (!tc::mbar_wait(bar + s, (kc >> 1) & 1, a.wait_cycles)) {
-        t0_fail = true;
+        atomicOr(&abort_flag, 1);
       } else {
         unsigned char* bHi = sB + s * bstage;
         unsigned char* bLo = bHi + tc::kSlices * a.N * 32;
@@ -426,8 +416,9 @@ __global__ void __launch_bounds__(tc::kThreads, 2) fj_mw_tc_kernel(MwTcDev a) {
         ++committed;
       }
     }
+    __syncthreads();
+    if (abort_flag) break;
   }
-  if (__syncthreads_or(t0_fail)) aborted = true;  // the last chunk's B wait
 
   // Drain: wait for the last committed MMA group (its commit covers every
   // earlier MMA of this thread) and, after an abort, for every B copy still
@@ -443,14 +434,14 @@ __global__ void __launch_bounds__(tc::kThreads, 2) fj_mw_tc_kernel(MwTcDev a) {
     const int last = n_committed - 1;
     if (!tc::mbar_wait(bar + 2 + (last & 1), (last >> 1) & 1, a.wait_cycles)) atomicOr(&drain_fail, 1);
   }
-  if (aborted && tid == 0) {
+  if (abort_flag && tid == 0) {
     for (int kc = n_committed; kc < n_issued; ++kc)
       if (!tc::mbar_wait(bar + (kc & 1), (kc >> 1) & 1, a.wait_cycles)) atomicOr(&drain_fail, 1);
   }
   tc::tc_fence_before();
   __syncthreads();
   tc::tc_fence_after();
-  if (!aborted && !drain_fail && n_committed == a.nchunks) {
+  if (!abort_flag && !drain_fail && n_committed == a.nchunks) {
     // epilogue: row `row` of accumulator `mh` -> |Re + i Im| / k^2
     const uint32_t tbase = tmem + ((uint32_t)(tid & 96) << 16) + (uint32_t)(mh * a.N);
     const int c = c0 + tid;
