@@ -347,8 +347,8 @@ static int split_for(const ccfj_fj_args& a, int cpt, int split_choice) {
 // Bytes of the itype-1 per-station geometry and per-frequency fold
 // thresholds, and of one input's interval data.
 size_t geometry_bytes(const ccfj_fj_args& a) { return sizeof(float4) * (size_t)a.nr; }
-size_t kbounds_bytes(const ccfj_fj_args& a) {  // fold and closed-fold thresholds
-  return a.itype == 1 ? 2 * (a.precision == CCFJ_PREC_FP32 ? 4 : 8) * (size_t)a.nf : 0;
+size_t kbounds_bytes(const ccfj_fj_args& a) {
+  return a.itype == 1 ? (a.precision == CCFJ_PREC_FP32 ? 4 : 8) * (size_t)a.nf : 0;
 }
 size_t interval_data_bytes(const ccfj_fj_args& a) {
   const size_t t = a.precision == CCFJ_PREC_FP32 ? 4 : 8;
@@ -364,17 +364,13 @@ int prep_interval_data(const ccfj_fj_args& a, FjDev& d, const InDesc* in, int ni
   const bool fp32 = a.precision == CCFJ_PREC_FP32;
   if (a.itype == 1) {
     const dim3 kbb(32, 8);
-    if (fp32) {
-      float* t = static_cast<float*>(kb);
-      fj_kbounds_kernel<float><<<div_up(a.nf, 8), kbb, 0, s>>>(a.f, a.c, a.nf, a.nc, d.tau, t,
-                                                               t + a.nf);
-      d.kcl = t + a.nf;
-    } else {
-      double* t = static_cast<double*>(kb);
+    if (fp32)
+      fj_kbounds_kernel<float><<<div_up(a.nf, 8), kbb, 0, s>>>(a.f, a.c, a.nf, a.nc, d.tau,
+                                                               static_cast<float*>(kb));
+    else
       fj_kbounds_kernel<double><<<div_up(a.nf, 8), kbb, 0, s>>>(a.f, a.c, a.nf, a.nc,
-                                                                (double)d.tau, t, t + a.nf);
-      d.kcl = t + a.nf;
-    }
+                                                                (double)d.tau,
+                                                                static_cast<double*>(kb));
     count_launch();
     CCFJ_LAUNCH_CHECK("fj_kbounds_kernel");
     d.kb = kb;
