@@ -333,10 +333,9 @@ int batch_device(const ccfj_batch_args& a, long long total, cudaStream_t s) {
   const float tau = a.tau > 0 ? a.tau : kDefaultTau32;
   float* kb = nullptr;
   if (a.itype == 1) {
-    kb = sc.get_n<float>(2 * (size_t)a.nf);  // fold and closed-fold thresholds
+    kb = sc.get_n<float>(a.nf);
     if (!kb) return CCFJ_ERR_ALLOC;
-    fj_kbounds_kernel<float><<<div_up(a.nf, 8), dim3(32, 8), 0, s>>>(a.f, a.c, a.nf, a.nc, tau, kb,
-                                                                     kb + a.nf);
+    fj_kbounds_kernel<float><<<div_up(a.nf, 8), dim3(32, 8), 0, s>>>(a.f, a.c, a.nf, a.nc, tau, kb);
     count_launch();
     CCFJ_LAUNCH_CHECK("fj_kbounds_kernel");
   }
@@ -351,7 +350,6 @@ int batch_device(const ccfj_batch_args& a, long long total, cudaStream_t s) {
     bd.base.gb[j] = g;
   }
   bd.base.kb = kb;
-  bd.base.kcl = kb ? kb + a.nf : nullptr;
   bd.base.geo = geo;
   bd.base.rs = a.r;
   bd.base.drs = drs;

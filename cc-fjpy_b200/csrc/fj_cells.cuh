@@ -220,10 +220,6 @@ struct FjDev {
   // itype 1: StationCoef<T> [nr][nf] per input; itype 0: g * w [nr][nf]
   const void* gb[2];
   const void* kb;    // itype 1: fold threshold per frequency (T), see fold_threshold
-  const void* kcl;   // itype 1: closed-fold threshold per frequency (T, tau / min k), or NULL
-  // Per frequency, which kernel sums it: 1 the closed-fold instantiation,
-  // 0 the plain one (NULL: the plain one, everywhere).
-  const unsigned char* cf_freq;
   const float* f;
   const float* c;
   float* out;
@@ -338,14 +334,10 @@ __device__ __forceinline__ StationCoef<T> station_coef(T g, T gl, T gr, bool has
   return {(T)((P1 * rd + P2) * w), (T)((P2 * rd + P3) * w), (T)(P3 * rd * w), g};
 }
 
-// Fold threshold per frequency (one warp per frequency), and (cthr, when
-// not NULL) the closed-fold threshold tau / min k: an interval at least that
-// long takes the closed form at every velocity of the frequency. thr <=
-// cthr, so no interval is in both folds.
+// Fold threshold per frequency (one warp per frequency).
 template <typename T>
 __global__ void fj_kbounds_kernel(const float* __restrict__ f, const float* __restrict__ c,
-                                  int nf, int nc, T tau, T* __restrict__ thr,
-                                  T* __restrict__ cthr) {
+                                  int nf, int nc, T tau, T* __restrict__ thr) {
   const int fi = blockIdx.x * blockDim.y + threadIdx.y;
   if (fi >= nf) return;
   const float fl = f[fi];
@@ -359,10 +351,7 @@ __global__ void fj_kbounds_kernel(const float* __restrict__ f, const float* __re
     lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
     hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
   }
-  if (threadIdx.x == 0) {
-    thr[fi] = fold_threshold<T>(lo, hi, tau);
-    if (cthr) cthr[fi] = tau / lo;
-  }
+  if (threadIdx.x == 0) thr[fi] = fold_threshold<T>(lo, hi, tau);
 }
 
 // Station geometry for the itype-1 kernels (see FjDev::geo).
@@ -530,50 +519,6 @@ __device__ __forceinline__ Acc2<T> explicit_interval(const Cell<T>& cell, bool e
   return Acc2<T>{{acc[0], acc[1]}};
 }
 
-// The term of an interval (A, B) that takes the closed form at every
-// velocity of its frequency (the closed fold), in the units of the folded
-// sums (output / gam), from the two stations' values y = Z / M (M = gam /
-// sqrt(r), with the stored sqrt(r), 1 at r = 0) and B = int_0^x Z0. With
-// w = r / sqrt(r), V = w y0 / k^2 - B / (k^3 gam) and W = w y1 (so that
-// r Z0 = gam w y0), the reference's (1/k^2) [g_A I0 + (b/k) I1],
-// I0 = [x Z1], I1 = x_B dx Z1(x_B) + [x Z0] - [B] (src/FJcpu.cpp:253-268),
-// is
-//     b (V_B - V_A) + (W_B (g_A + b D) - g_A W_A) / k.
-// Each station's V and W serve both of its intervals, so B is evaluated
-// once per station instead of twice per interval.
-template <int MODE, typename T>
-__device__ __forceinline__ Acc2<T> closed_fold_interval(const Cell<T>& cell, T D, T rA, T sqA,
-                                                        T rB, T sqB, const ZB<T>& yAJ,
-                                                        const ZB<T>& yBJ, const ZB<T>& yAY,
-                                                        const ZB<T>& yBY, T gA0, T gB0, T gA1,
-                                                        T gB1) {
-  using fjs::fmaT;
-  const T ik = cell.inv_k, ik2 = cell.inv_k2;
-  const T ik3g = ik2 * ik / cell.gamma();
-  const T wA = rA / sqA, wB = rB / sqB;
-  auto term = [&](const ZB<T>& yA, const ZB<T>& yB, T gA, T gB) {
-    const T b = interval_slope<T>(gA, gB, (float)D);
-    const T VA = fmaT(wA * yA.z0, ik2, -(yA.b * ik3g));
-    const T VB = fmaT(wB * yB.z0, ik2, -(yB.b * ik3g));
-    const T WA = wA * yA.z1, WB = wB * yB.z1;
-    return fmaT(b, VB - VA, ik * fmaT(WB, fmaT(b, D, gA), -(gA * WA)));
-  };
-  T J0 = T(0), J1 = T(0), Y0 = T(0), Y1 = T(0);
-  if (ModeTraits<MODE>::WJ) {
-    J0 = term(yAJ, yBJ, gA0, gB0);
-    if (ModeTraits<MODE>::NIN > 1) J1 = term(yAJ, yBJ, gA1, gB1);
-  }
-  if (ModeTraits<MODE>::WY) {
-    Y0 = term(yAY, yBY, gA0, gB0);
-    if (ModeTraits<MODE>::NIN > 1) Y1 = term(yAY, yBY, gA1, gB1);
-  }
-  if (MODE == CCFJ_MODE_J) return Acc2<T>{{J0, T(0)}};
-  if (MODE == CCFJ_MODE_Y) return Acc2<T>{{Y0, T(0)}};
-  if (MODE == CCFJ_MODE_J_MINUS_Y) return Acc2<T>{{J0 - Y1, T(0)}};
-  if (MODE == CCFJ_MODE_ABS_J) return Acc2<T>{{J0, J1}};
-  return Acc2<T>{{J0 - Y1, J1 + Y0}};  // ABS_H: (J(u0) - Y(u1)) + i (J(u1) + Y(u0))
-}
-
 // Minimum resident 256-thread CTAs per SM of the kernels built on
 // fj_cells. FP32: three CTAs, at most 85 registers. Two velocities per
 // thread (the paired x >= 8 step) then fit without spilling; under four
@@ -680,11 +625,7 @@ struct PairedStationJ<true> {
 // CPT cells (f, c), (f, c + 1), ... per thread share the per-station loads.
 // The transform of the CPT cells (fi, c0), (fi, c0 + 1), ... of one data
 // set; shared by the grid kernel below and the persistent batch kernel.
-// CF: the closed-fold instantiation (itype 1; a.kcl required), which sums
-// an interval at least tau / min k long from the stations' carried values
-// instead of the explicit path. Either instantiation stores only the
-// frequencies a.cf_freq gives it.
-template <int MODE, int ITYPE, typename T, int CPT, bool CF = false>
+template <int MODE, int ITYPE, typename T, int CPT>
 __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
   using MT = ModeTraits<MODE>;
   constexpr bool WJ = MT::WJ, WY = MT::WY;
@@ -709,9 +650,6 @@ __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
   for (int j = 0; j < CPT; ++j) tot[j][0] = tot[j][1] = T(0);
   if constexpr (ITYPE == 1) {
     const T thr_fold = static_cast<const T*>(a.kb)[fi];
-    // closed-fold threshold tau / min k (none without a table)
-    T cthr = T(0);
-    if constexpr (CF) cthr = static_cast<const T*>(a.kcl)[fi];
     const StationCoef<T>* q0p = static_cast<const StationCoef<T>*>(a.gb[0]) + fi;
     const StationCoef<T>* q1p = static_cast<const StationCoef<T>*>(a.gb[MT::NIN > 1 ? 1 : 0]) + fi;
     const T d8 = T(8) / (T)a.tau;  // closed form where |D| d8 >= s8 (k |D| >= tau)
@@ -735,10 +673,10 @@ __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
     // evaluate station i-1 again when an explicit interval comes.
     constexpr bool kCarry = !(WJ && WY);
     ZB<T> zpJ[kCarry ? CPT : 1], zpY[kCarry ? CPT : 1];
-    // State of interval (i-1, i): length D, folded in, in the closed fold,
-    // reaches near the origin. Station 0 has no such interval.
+    // State of interval (i-1, i): length D, folded in, reaches near the
+    // origin. Station 0 has no such interval.
     T D = T(0);
-    bool fold_cur = true, cf_cur = false, near_cur = false;
+    bool fold_cur = true, near_cur = false;
     T acc0[CPT][2], acc1[CPT][2];
     // One station: out += gam (y0 (A - k^2 C) - k y1 B), plus the explicit
     // interval (i-1, i) where it is not (only) in the folded sum.
@@ -748,8 +686,6 @@ __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
       const T r = gm.x, D_next = gm.y;
       const long long qi = (long long)i * a.nf;
       const T dl8 = fabs(D) * d8;
-      bool cf_next = false;
-      if constexpr (CF) cf_next = fabs(D_next) >= cthr;
       ZB<T> Jzs[CPT], Yzs[CPT];
 #if defined(FJS_HAVE_PAIRED)
       if constexpr (kPaired && LARGE) {
@@ -776,10 +712,7 @@ __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
         ZB<T> Jz = Jzs[j], Yz = Yzs[j];
         const bool clJ = dl8 >= cell[j].s8;
         const bool clY = clJ || near_cur;  // Y0 is singular at 0
-        // an interval in the closed fold is not explicit (below)
-        const bool exJ = WJ && !(CF && cf_cur) && (clJ || !fold_cur);
-        const bool exY = WY && !(CF && cf_cur) && (clY || !fold_cur);
-        bool bdone = false;  // B of this station evaluated
+        const bool exJ = WJ && (clJ || !fold_cur), exY = WY && (clY || !fold_cur);
         if (i > 0 && (exJ || exY)) {
           const float4 gp = __ldg(a.geo + i - 1);
           ZB<T> pJ{}, pY{};
@@ -793,7 +726,6 @@ __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
           if ((WJ && exJ && clJ) || (WY && exY && clY)) {
             cell[j].template fill_b<WJ, WY>((T)gp.x, (T)gp.z, pJ, pY);
             cell[j].template fill_b<WJ, WY>(r, (T)gm.z, Jz, Yz);
-            bdone = true;
           }
           const T gA0 = __ldg(&q0p[qi - a.nf].g);
           const T gA1 = MT::NIN > 1 ? __ldg(&q1p[qi - a.nf].g) : T(0);
@@ -803,38 +735,11 @@ __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
           acc0[j][0] += e.v[0];
           acc0[j][1] += e.v[1];
         }
-        // Closed fold: B of this station where an interval on either side is
-        // in it (single-basis modes carry it to the next station; two-basis
-        // modes evaluate the previous station again), and the term of the
-        // interval (i-1, i) from both stations' values.
-        if constexpr (CF) {
-        if ((kCarry ? (cf_cur || cf_next) : cf_cur) && !bdone)
-          cell[j].template fill_b<WJ, WY>(r, (T)gm.z, Jz, Yz);
-        if (i > 0 && cf_cur) {
-          const float4 gp = __ldg(a.geo + i - 1);
-          ZB<T> pJ{}, pY{};
-          if constexpr (kCarry) {
-            pJ = zpJ[j];
-            pY = zpY[j];
-          } else {
-            cell[j].template eval_y<WJ, WY, false>((T)gp.x, (T)gp.z, (T)gp.w, pJ, pY);
-            cell[j].template fill_b<WJ, WY>((T)gp.x, (T)gp.z, pJ, pY);
-          }
-          const T gA0 = __ldg(&q0p[qi - a.nf].g);
-          const T gA1 = MT::NIN > 1 ? __ldg(&q1p[qi - a.nf].g) : T(0);
-          const Acc2<T> e = closed_fold_interval<MODE, T>(cell[j], D, (T)gp.x, (T)gp.w, r,
-                                                          (T)gm.w, pJ, Jz, pY, Yz, gA0, q0.g, gA1,
-                                                          q1.g);
-          acc0[j][0] += e.v[0];
-          acc0[j][1] += e.v[1];
-        }
-        }  // CF
         if constexpr (kCarry) {
           if (WJ) zpJ[j] = Jz;
           if (WY) zpY[j] = Yz;
         }
       }
-      if constexpr (CF) cf_cur = cf_next;
       fold_cur = folded_interval<T>(thr_fold, D_next, r);
       near_cur = D_next > r;
       D = D_next;
@@ -846,14 +751,11 @@ __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
       const float4 gp = __ldg(a.geo + a.i_lo - 1);
       D = (T)gp.y;
       fold_cur = folded_interval<T>(thr_fold, D, (T)gp.x);
-      if constexpr (CF) cf_cur = fabs(D) >= cthr;
       near_cur = D > (T)gp.x;
       if constexpr (kCarry) {
 #pragma unroll
-        for (int j = 0; j < CPT; ++j) {
+        for (int j = 0; j < CPT; ++j)
           cell[j].template eval_y<WJ, WY, false>((T)gp.x, (T)gp.z, (T)gp.w, zpJ[j], zpY[j]);
-          if (CF && cf_cur) cell[j].template fill_b<WJ, WY>((T)gp.x, (T)gp.z, zpJ[j], zpY[j]);
-        }
       }
     }
     const int lane = threadIdx.x & 31;
@@ -952,12 +854,10 @@ __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
       }
     }
     if (!c_valid) return;
-    // this instantiation's frequencies only
-    const bool own = !a.cf_freq || ((a.cf_freq[fi] != 0) == CF);
     if (a.part) {  // raw sums of this station range
 #pragma unroll
       for (int j = 0; j < CPT; ++j)
-        if (f_valid && own && c0 + j < a.nc)
+        if (f_valid && c0 + j < a.nc)
 #pragma unroll
           for (int q = 0; q < MT::NACC; ++q)
             a.part[((long long)q * a.nc + c0 + j) * a.nf + fi] = (float)tot[j][q];
@@ -971,7 +871,7 @@ __device__ __forceinline__ void fj_cells(const FjDev& a, int fi, int c0) {
       res[1] = gam * tot[j][1];
       // k = 0 (f = 0) divides by zero in the reference: NaN
       const float v = cell[j].k == T(0) ? __int_as_float(0x7fffffff) : finish<MODE, T>(res, T(1));
-      if (f_valid && own && c0 + j < a.nc) a.out[(long long)(c0 + j) * a.nf + fi] = v;
+      if (f_valid && c0 + j < a.nc) a.out[(long long)(c0 + j) * a.nf + fi] = v;
     }
   } else {
     // Trapezoid: out = gam sum_s y0(x_s) q_s with y0 = Z0 / M and the

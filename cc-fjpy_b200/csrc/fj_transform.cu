@@ -59,15 +59,8 @@ __global__ void fj_prep_geom_kernel(const float* __restrict__ rs, int nr, float*
   wtr[i] = (w0 + w1) * 0.5f * r;
 }
 
-template <int MODE, int ITYPE, typename T, int CPT, bool CF = false>
+template <int MODE, int ITYPE, typename T, int CPT>
 __global__ void __launch_bounds__(256, fj_min_blocks<T>()) fj_amortized_kernel(FjDev a) {
-  if (a.cf_freq) {
-    // both instantiations run over every frequency tile: a CTA goes on only
-    // if one of its 32 frequencies is this instantiation's (every warp holds
-    // the same 32 frequencies, so the vote is the same in all of them)
-    const int f = min((int)(blockIdx.y * blockDim.x + threadIdx.x), a.nf - 1);
-    if (!__any_sync(0xffffffffu, (a.cf_freq[f] != 0) == CF)) return;
-  }
   if (gridDim.z > 1) {
     // split launch: CTA layer z sums stations [z L, (z + 1) L) into its own
     // partial sums (fj_split_finish_kernel adds the layers in order)
@@ -77,28 +70,8 @@ __global__ void __launch_bounds__(256, fj_min_blocks<T>()) fj_amortized_kernel(F
   }
   // velocity tiles on grid x: the CTAs of one frequency tile run side by
   // side and share its station coefficients in L2
-  fj_cells<MODE, ITYPE, T, CPT, CF>(a, blockIdx.y * blockDim.x + threadIdx.x,
-                                    (blockIdx.x * blockDim.y + threadIdx.y) * CPT);
-}
-
-// Which frequencies the closed-fold instantiation takes: those where at
-// least 1/16 of the intervals are at least tau / min k long (cthr), so take
-// the closed form at every velocity. One CTA per frequency, the intervals
-// counted over its threads.
-__global__ void fj_cf_freq_kernel(const float* __restrict__ drs, int nr,
-                                  const float* __restrict__ cthr, int nf,
-                                  unsigned char* __restrict__ cf_freq) {
-  __shared__ int count;
-  const int f = blockIdx.x;
-  if (threadIdx.x == 0) count = 0;
-  __syncthreads();
-  const float t = cthr[f];
-  int n = 0;
-  for (int i = 1 + threadIdx.x; i < nr; i += blockDim.x) n += fabsf(drs[i]) >= t;
-  for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
-  if ((threadIdx.x & 31) == 0) atomicAdd(&count, n);
-  __syncthreads();
-  if (threadIdx.x == 0) cf_freq[f] = 16 * count >= nr - 1 && nr > 1;
+  fj_cells<MODE, ITYPE, T, CPT>(a, blockIdx.y * blockDim.x + threadIdx.x,
+                                (blockIdx.x * blockDim.y + threadIdx.y) * CPT);
 }
 
 // Sum of the station ranges of a split launch, in range order (the result
@@ -254,15 +227,6 @@ void launch_amortized_cpt(int itype, const FjDev& d, cudaStream_t s) {
     fj_amortized_kernel<MODE, 1, T, CPT><<<grid, block, 0, s>>>(d);
   else
     fj_amortized_kernel<MODE, 0, T, CPT><<<grid, block, 0, s>>>(d);
-  if constexpr (sizeof(T) == 4) {
-    // the closed-fold frequencies: one velocity per thread (the carried B
-    // and the closed-fold terms fit the register bound without spilling)
-    if (itype == 1 && d.cf_freq) {
-      count_launch();
-      const dim3 grid1(div_up(d.nc, 8), div_up(d.nf, 32), nsplit);
-      fj_amortized_kernel<MODE, 1, float, 1, true><<<grid1, block, 0, s>>>(d);
-    }
-  }
 }
 
 template <int MODE, typename T>
@@ -383,8 +347,8 @@ static int split_for(const ccfj_fj_args& a, int cpt, int split_choice) {
 // Bytes of the itype-1 per-station geometry and per-frequency fold
 // thresholds, and of one input's interval data.
 size_t geometry_bytes(const ccfj_fj_args& a) { return sizeof(float4) * (size_t)a.nr; }
-size_t kbounds_bytes(const ccfj_fj_args& a) {  // fold and closed-fold thresholds
-  return a.itype == 1 ? 2 * (a.precision == CCFJ_PREC_FP32 ? 4 : 8) * (size_t)a.nf : 0;
+size_t kbounds_bytes(const ccfj_fj_args& a) {
+  return a.itype == 1 ? (a.precision == CCFJ_PREC_FP32 ? 4 : 8) * (size_t)a.nf : 0;
 }
 size_t interval_data_bytes(const ccfj_fj_args& a) {
   const size_t t = a.precision == CCFJ_PREC_FP32 ? 4 : 8;
@@ -400,17 +364,13 @@ int prep_interval_data(const ccfj_fj_args& a, FjDev& d, const InDesc* in, int ni
   const bool fp32 = a.precision == CCFJ_PREC_FP32;
   if (a.itype == 1) {
     const dim3 kbb(32, 8);
-    if (fp32) {
-      float* t = static_cast<float*>(kb);
-      fj_kbounds_kernel<float><<<div_up(a.nf, 8), kbb, 0, s>>>(a.f, a.c, a.nf, a.nc, d.tau, t,
-                                                               t + a.nf);
-      d.kcl = t + a.nf;
-    } else {
-      double* t = static_cast<double*>(kb);
+    if (fp32)
+      fj_kbounds_kernel<float><<<div_up(a.nf, 8), kbb, 0, s>>>(a.f, a.c, a.nf, a.nc, d.tau,
+                                                               static_cast<float*>(kb));
+    else
       fj_kbounds_kernel<double><<<div_up(a.nf, 8), kbb, 0, s>>>(a.f, a.c, a.nf, a.nc,
-                                                                (double)d.tau, t, t + a.nf);
-      d.kcl = t + a.nf;
-    }
+                                                                (double)d.tau,
+                                                                static_cast<double*>(kb));
     count_launch();
     CCFJ_LAUNCH_CHECK("fj_kbounds_kernel");
     d.kb = kb;
@@ -511,16 +471,6 @@ int fj_device(const ccfj_fj_args& a, cudaStream_t s, int cpt_choice, int split_c
     }
     const int st = prep_interval_data(a, d, in, nin, kb, gbuf, wtr, s);
     if (st != CCFJ_OK) return st;
-    if (a.itype == 1 && a.precision == CCFJ_PREC_FP32 && a.nr > 1) {
-      // the frequencies whose long intervals go to the closed-fold kernel
-      unsigned char* cf = sc.get_n<unsigned char>(a.nf);
-      if (!cf) return CCFJ_ERR_ALLOC;
-      fj_cf_freq_kernel<<<a.nf, 256, 0, s>>>(drs, a.nr, static_cast<const float*>(d.kcl), a.nf,
-                                             cf);
-      count_launch();
-      CCFJ_LAUNCH_CHECK("fj_cf_freq_kernel");
-      d.cf_freq = cf;
-    }
   }
 
   const int cpt = variant_for(a, cpt_choice);
