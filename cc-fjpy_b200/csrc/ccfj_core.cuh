@@ -77,6 +77,11 @@ class Scratch {
 // bytes; kind 1: `n` floats stored as doubles. Large copies run through
 // pinned staging buffers on several host threads (host_copy.cu).
 int copy_to_host(void* dst, const void* dsrc, size_t n, int kind, cudaStream_t s);
+// Copies n bytes of input from host memory to device memory ddst, ordered
+// after the work queued on s. A large copy from pageable memory runs
+// through the same staging on several host threads and is complete on
+// return; other copies are queued on s (cudaMemcpyAsync).
+int copy_from_host(void* ddst, const void* src, size_t n, cudaStream_t s);
 
 // Optional event timer around the main transform kernel (ccfj_profile_enable).
 void prof_begin(cudaStream_t s);

@@ -619,7 +619,10 @@ int batch_host(const ccfj_batch_args& a, cudaStream_t s) {
   float* dout = sc.get_n<float>((size_t)a.nsets * a.nc * a.nf);
   long long* dp = a.perm ? sc.get_n<long long>(total) : nullptr;
   if (!du || !doff || !dr || !df || !dc || !dout || (a.perm && !dp)) return CCFJ_ERR_ALLOC;
-  if (ng == 0) CCFJ_CUDA_TRY(cudaMemcpyAsync(du, lo, ubytes, cudaMemcpyHostToDevice, s));
+  if (ng == 0) {
+    const int cst = copy_from_host(du, lo, ubytes, s);
+    if (cst != CCFJ_OK) return cst;
+  }
   CCFJ_CUDA_TRY(cudaMemcpyAsync(doff, off, sizeof(long long) * (a.nsets + 1), cudaMemcpyHostToDevice, s));
   CCFJ_CUDA_TRY(cudaMemcpyAsync(dr, a.r, sizeof(float) * total, cudaMemcpyHostToDevice, s));
   CCFJ_CUDA_TRY(cudaMemcpyAsync(df, a.f, sizeof(float) * a.nf, cudaMemcpyHostToDevice, s));

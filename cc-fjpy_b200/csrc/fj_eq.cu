@@ -154,7 +154,8 @@ static int eq_host(const ccfj_eq_args& a, cudaStream_t s) {
   unsigned int* derr = sc.get_n<unsigned int>(1);
   if (!du || !dr || !df || !dc || !dout || !derr) return CCFJ_ERR_ALLOC;
   CCFJ_CUDA_TRY(cudaMemsetAsync(derr, 0, sizeof(unsigned int), s));
-  CCFJ_CUDA_TRY(cudaMemcpyAsync(du, a.u, ubytes, cudaMemcpyHostToDevice, s));
+  int cst = copy_from_host(du, a.u, ubytes, s);
+  if (cst != CCFJ_OK) return cst;
   CCFJ_CUDA_TRY(cudaMemcpyAsync(dr, a.r, sizeof(float) * a.ntr, cudaMemcpyHostToDevice, s));
   CCFJ_CUDA_TRY(cudaMemcpyAsync(df, a.f, sizeof(float) * a.nf, cudaMemcpyHostToDevice, s));
   CCFJ_CUDA_TRY(cudaMemcpyAsync(dc, a.c, sizeof(float) * a.nc, cudaMemcpyHostToDevice, s));

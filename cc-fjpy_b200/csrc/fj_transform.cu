@@ -871,13 +871,15 @@ static int fj_host(const ccfj_fj_args& a, cudaStream_t s) {
   if (merged) {
     float* du = sc.get_n<float>(hi - lo);
     if (!du) return CCFJ_ERR_ALLOC;
-    CCFJ_CUDA_TRY(cudaMemcpyAsync(du, lo, sizeof(float) * (hi - lo), cudaMemcpyHostToDevice, s));
+    const int cst = copy_from_host(du, lo, sizeof(float) * (hi - lo), s);
+    if (cst != CCFJ_OK) return cst;
     for (int j = 0; j < nin; ++j) d.u[j] = du + (a.u[j] - lo);
   } else {
     for (int j = 0; j < nin; ++j) {
       float* du = sc.get_n<float>(span);
       if (!du) return CCFJ_ERR_ALLOC;
-      CCFJ_CUDA_TRY(cudaMemcpyAsync(du, a.u[j], sizeof(float) * span, cudaMemcpyHostToDevice, s));
+      const int cst = copy_from_host(du, a.u[j], sizeof(float) * span, s);
+      if (cst != CCFJ_OK) return cst;
       d.u[j] = du;
     }
   }

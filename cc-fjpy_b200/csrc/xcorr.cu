@@ -254,7 +254,8 @@ static int run(const ccfj_cc_args& a, cudaStream_t s) {
   if (!a.device_ptrs) {
     float* d = sc.get_n<float>(nrec);
     if (!d) return CCFJ_ERR_ALLOC;
-    CCFJ_CUDA_TRY(cudaMemcpyAsync(d, a.data, nrec * sizeof(float), cudaMemcpyHostToDevice, s));
+    const int cst = copy_from_host(d, a.data, nrec * sizeof(float), s);
+    if (cst != CCFJ_OK) return cst;
     d_data = d;
   }
   // outputs: planes (re, im) [npairs][nf] or interleaved complex [npairs][nf]
@@ -421,7 +422,8 @@ static int cc_fj_noise(const ccfj_cc_args& cc, const ccfj_fj_args& fj, cudaStrea
                  cc.npts);
     float* d = sc.get_n<float>(nrec);
     if (!d) return CCFJ_ERR_ALLOC;
-    CCFJ_CUDA_TRY(cudaMemcpyAsync(d, cc.data, nrec * sizeof(float), cudaMemcpyHostToDevice, s));
+    const int cst = copy_from_host(d, cc.data, nrec * sizeof(float), s);
+    if (cst != CCFJ_OK) return cst;
     c.data = d;
   }
   ccfj_fj_args f = fj;

@@ -1,4 +1,5 @@
-"""Large results copied to host memory (csrc/host_copy.cu).
+"""Large results and inputs copied between host memory and the device
+(csrc/host_copy.cu).
 
 Results of 16 MiB and more go to pageable host memory through pinned
 staging buffers on several host threads; MWFJ's float64 result is converted
@@ -6,8 +7,10 @@ on the way. Checked here: the staged copy equals the device result read by
 torch bit for bit, MWFJ's float64 result is exactly its float32 result
 widened (staged and unstaged sizes), two calls that overlap on the host
 (one takes the staging buffers, the other the plain route) both come back
-right, and a batch of 256 MB or more of host spectra, run in groups of sets
-with the copies overlapping the transforms, equals one device-resident pass.
+right, a batch of 256 MB or more of host spectra, run in groups of sets
+with the copies overlapping the transforms, equals one device-resident pass,
+and large pageable inputs, staged the other way round, give the same bits as
+pinned ones.
 """
 import ctypes
 import threading
@@ -111,6 +114,27 @@ def test_mwfj_double_result_is_the_float_result_widened(nwin, nc):
         y32 = _eq._run(u, r, c, f, 1, 1, 0, nwin=nwin, wins=wins)
     assert y.dtype == np.float64 and y32.dtype == np.float32 and y.shape == (nwin, nc, nf)
     assert np.array_equal(y, y32.astype(np.float64), equal_nan=True)
+
+
+def test_staged_input_equals_pinned_input():
+    """20 MB of pageable traces reach the device through the threads'
+    pinned staging; the same traces in pinned memory go in one plain copy.
+    fj_earthquake gives the same bits either way."""
+    import ccfj
+    rng = np.random.default_rng(31)
+    ntr, npts, Fs = 640, 8192, 20.0
+    r = np.exp(rng.uniform(np.log(1e4), np.log(2e6), ntr))
+    u = cases.ricker_records(rng, r, npts, Fs)
+    assert u.dtype == np.float32 and u.nbytes >= 8 << 20
+    f = Fs * np.arange(256) / npts
+    c = np.linspace(2000.0, 5000.0, 64)
+    pinned = ccfj.pinned_empty(u.shape, np.float32)
+    pinned[...] = u
+    with warnings.catch_warnings():
+        warnings.simplefilter("ignore")
+        y_pageable = ccfj.fj_earthquake(u, r, c, f)
+        y_pinned = ccfj.fj_earthquake(pinned, r, c, f)
+    assert np.array_equal(y_pageable, y_pinned, equal_nan=True)
 
 
 def test_overlapping_host_calls():
