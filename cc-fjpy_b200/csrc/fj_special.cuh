@@ -477,25 +477,42 @@ struct PairPhase {
   float2 qhi, nqhi, qlo, s8;
 };
 
+// sincos_cycles_f32(chi_cycles_f32(p_hi, p_lo)) of both lanes: the
+// reduction to cycles (the magic-number rounding and the sums after it) and
+// the 2 pi scaling are round-to-nearest adds and a multiply, so the paired
+// forms give each lane's bits; the sine and cosine stay per lane.
+__device__ __forceinline__ void sincos_cycles_pair(float2 p_hi, float2 p_lo, float2& sn,
+                                                   float2& cs) {
+  const float kMagic = 12582912.0f;  // as chi_cycles_f32
+  const float2 n = padd(padd(p_hi, psplat(kMagic)), psplat(-kMagic));
+  const float2 u = padd(pfma(psplat(-1.0f), n, p_hi), padd(p_lo, psplat(-0.125f)));
+#ifdef __CUDA_ARCH__
+  const float2 arg = pmul(psplat(kTwoPiF), u);
+  asm("sin.approx.ftz.f32 %0, %1;" : "=f"(sn.x) : "f"(arg.x));
+  asm("cos.approx.ftz.f32 %0, %1;" : "=f"(cs.x) : "f"(arg.x));
+  asm("sin.approx.ftz.f32 %0, %1;" : "=f"(sn.y) : "f"(arg.y));
+  asm("cos.approx.ftz.f32 %0, %1;" : "=f"(cs.y) : "f"(arg.y));
+#else
+  sincos_cycles_f32(u.x, sn.x, cs.x);
+  sincos_cycles_f32(u.y, sn.y, cs.y);
+#endif
+}
+
 // eval_large_scaled_f32<true, false, true> (need_b false) of both lanes at
 // the station r (1/r = rinv): y0 = J0 / M and y1 = J1 / M, x >= 8 in both.
 __device__ __forceinline__ void eval_large_scaled_pair_j(const PairPhase& ph, float r, float rinv,
                                                          ZB2& J) {
-  // The phase in cycles, per lane with the scalar code (p_hi = q_hi r,
-  // p_lo = fma(q_lo, r, fma(q_hi, r, -p_hi)), chi_cycles_f32): written with
-  // paired operations it measured about 2e-3 rad less accurate at x = 3e4,
-  // as if the low part of the double-float phase had been lost.
+  // The double-float phase in cycles, per lane with the scalar code (p_hi =
+  // q_hi r, p_lo = fma(q_lo, r, fma(q_hi, r, -p_hi))): written with paired
+  // operations it measured about 2e-3 rad less accurate at x = 3e4, as if
+  // the low part had been lost. Its reduction to cycles is paired.
+  float2 p_hi, p_lo;
+  p_hi.x = ph.qhi.x * r;
+  p_lo.x = fmaf(ph.qlo.x, r, fmaf(ph.qhi.x, r, -p_hi.x));
+  p_hi.y = ph.qhi.y * r;
+  p_lo.y = fmaf(ph.qlo.y, r, fmaf(ph.qhi.y, r, -p_hi.y));
   float2 sn, cs;
-  {
-    const float p_hi = ph.qhi.x * r;
-    const float p_lo = fmaf(ph.qlo.x, r, fmaf(ph.qhi.x, r, -p_hi));
-    sincos_cycles_f32(chi_cycles_f32(p_hi, p_lo), sn.x, cs.x);
-  }
-  {
-    const float p_hi = ph.qhi.y * r;
-    const float p_lo = fmaf(ph.qlo.y, r, fmaf(ph.qhi.y, r, -p_hi));
-    sincos_cycles_f32(chi_cycles_f32(p_hi, p_lo), sn.y, cs.y);
-  }
+  sincos_cycles_pair(p_hi, p_lo, sn, cs);
   const float2 sv = pmul(ph.s8, psplat(rinv));  // s = 8 / x
   const float2 z = pmul(sv, sv);
   constexpr float cp0[] = FJC_F32_L_P0;
@@ -517,8 +534,7 @@ __device__ __forceinline__ void eval_large_scaled_pair_j(const PairPhase& ph, fl
 __device__ __forceinline__ void eval_large_pair_stations_j(float2 x, float2 p_hi, float2 p_lo,
                                                            bool need_b, ZB2& J, float2& B) {
   float2 sn, cs;
-  sincos_cycles_f32(chi_cycles_f32(p_hi.x, p_lo.x), sn.x, cs.x);
-  sincos_cycles_f32(chi_cycles_f32(p_hi.y, p_lo.y), sn.y, cs.y);
+  sincos_cycles_pair(p_hi, p_lo, sn, cs);
   const float2 rs = make_float2(rsqrt_fast(x.x), rsqrt_fast(x.y));
   const float2 M = pmul(psplat(kSqrt2OverPiF), rs);
   const float2 s = pmul(psplat(8.0f), pmul(rs, rs));
