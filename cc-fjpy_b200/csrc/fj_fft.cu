@@ -228,13 +228,18 @@ __device__ __forceinline__ void twiddle_powers(const float2* __restrict__ tw, in
 }
 
 // One Stockham pass of radix R over the 16 registers of thread tid (16/R
-// butterflies j = tid + g P), writing the outputs to shared memory.
+// butterflies j = tid + g P), writing the outputs to shared memory. In the
+// last pass (Ns R = M) butterfly j writes outputs j + r Ns; one none of
+// whose outputs is at most kneed or at least M - kneed is skipped (the
+// real-FFT split reads only those).
 template <int R>
 __device__ __forceinline__ void stockham_pass(float2 (&v)[16], float2* sz, int M, int Ns,
-                                              const float2* __restrict__ tw, int tid, int P) {
+                                              const float2* __restrict__ tw, int tid, int P,
+                                              int kneed) {
 #pragma unroll
   for (int g = 0; g < 16 / R; ++g) {
     const int j = tid + g * P;
+    if (Ns * R == M && j > kneed && j + (R - 1) * Ns < M - kneed) continue;
     const int k = j % Ns;
     float2* u = v + g * R;
     if (Ns > 1) {
@@ -264,10 +269,12 @@ __device__ __forceinline__ void stockham_load(float2 (&v)[16], const float2* sz,
 
 // The whole M-point FFT of the 16 points per thread in v (the first pass's
 // inputs, in[tid + r P]); the result is left in natural order in sz (padded
-// indices) and the CTA is synchronised.
+// indices) and the CTA is synchronised. Only outputs at most kneed or at
+// least M - kneed are guaranteed (kneed >= M: all of them).
 __device__ __forceinline__ void stockham_fft(float2 (&v)[16], float2* sz, int M,
-                                             const float2* __restrict__ tw, int tid, int P) {
-  stockham_pass<16>(v, sz, M, 1, tw, tid, P);
+                                             const float2* __restrict__ tw, int tid, int P,
+                                             int kneed) {
+  stockham_pass<16>(v, sz, M, 1, tw, tid, P, kneed);
   __syncthreads();
   int Ns = 16;
   while (Ns < M) {
@@ -275,22 +282,22 @@ __device__ __forceinline__ void stockham_fft(float2 (&v)[16], float2* sz, int M,
     if (rem >= 16) {
       stockham_load<16>(v, sz, M, tid, P);
       __syncthreads();
-      stockham_pass<16>(v, sz, M, Ns, tw, tid, P);
+      stockham_pass<16>(v, sz, M, Ns, tw, tid, P, kneed);
       Ns *= 16;
     } else if (rem == 8) {
       stockham_load<8>(v, sz, M, tid, P);
       __syncthreads();
-      stockham_pass<8>(v, sz, M, Ns, tw, tid, P);
+      stockham_pass<8>(v, sz, M, Ns, tw, tid, P, kneed);
       Ns *= 8;
     } else if (rem == 4) {
       stockham_load<4>(v, sz, M, tid, P);
       __syncthreads();
-      stockham_pass<4>(v, sz, M, Ns, tw, tid, P);
+      stockham_pass<4>(v, sz, M, Ns, tw, tid, P, kneed);
       Ns *= 4;
     } else {
       stockham_load<2>(v, sz, M, tid, P);
       __syncthreads();
-      stockham_pass<2>(v, sz, M, Ns, tw, tid, P);
+      stockham_pass<2>(v, sz, M, Ns, tw, tid, P, kneed);
       Ns *= 2;
     }
     __syncthreads();
@@ -335,7 +342,9 @@ __global__ void __launch_bounds__(kStockMaxM / 16, 2)
 #pragma unroll
     for (int r = 0; r < 16; ++r) v[r] = __ldg(x + tid + r * P);
   }
-  stockham_fft(v, sz, M, tw, tid, P);
+  // the split below reads bins up to (nbins - 1) bin_stride and their mirrors
+  const long long kmax = (long long)(job.nbins - 1) * job.bin_stride;
+  stockham_fft(v, sz, M, tw, tid, P, kmax < M ? (int)kmax : M);
   // real-transform split, bins k < nbins (k <= M)
   float2* out = job.out + (long long)row * job.nbins;
   for (int kk = tid; kk < job.nbins; kk += P) {
@@ -376,7 +385,7 @@ __global__ void __launch_bounds__(kStockMaxM / 16, 2)
     const long long m = tid + r * P;
     v[r] = make_float2(xa[m * es], has_b ? xb[m * es] : 0.0f);
   }
-  stockham_fft(v, sz, M, tw, tid, P);
+  stockham_fft(v, sz, M, tw, tid, P, M);
   const int h = M >> 1;
 #pragma unroll
   for (int r = 0; r < 16; ++r) {
@@ -388,7 +397,7 @@ __global__ void __launch_bounds__(kStockMaxM / 16, 2)
                               : make_float2(z.y, z.x);
   }
   __syncthreads();  // every read of Z is done before the second FFT writes sz
-  stockham_fft(v, sz, M, tw, tid, P);
+  stockham_fft(v, sz, M, tw, tid, P, M);
   const float inv_n = 1.0f / (float)n;
   for (int j = tid; j < n; j += P) {
     if (j % fstride) continue;
