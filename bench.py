@@ -813,6 +813,10 @@ def measure_batch(lib, torch, dev, sp, peak, args):
     o64 = torch.empty((nc, nf), device="cuda")
     errs = []
     nan_ok = True
+    # the subarrays the CPU sample covers (stratified by size); their FP64
+    # form is kept to judge FJcpu.cpp on the same columns
+    picks = np.argsort(counts)[np.linspace(0, nsets - 1, 8).round().astype(int)]
+    y64_picked = {}
     t0 = time.perf_counter()
     for b in range(nsets):
         a = single[b]
@@ -821,6 +825,8 @@ def measure_batch(lib, torch, dev, sp, peak, args):
         y64b = o64.cpu().numpy()
         errs.append(_err(y32[b], y64b))
         nan_ok &= _nan_equal(y32[b], y64b)
+        if b in picks:
+            y64_picked[int(b)] = y64b
     t64 = time.perf_counter() - t0
     terms = total * nf * nc
     # end to end: host spectra in pinned memory, one view per subarray
@@ -852,12 +858,12 @@ def measure_batch(lib, torch, dev, sp, peak, args):
                                                                                         t64),
                      "e2e_equals_device": e2e_eq},
     }
-    # host copies of the subarrays the CPU sample covers (stratified by size)
-    picks = np.argsort(counts)[np.linspace(0, nsets - 1, 8).round().astype(int)]
+    # host copies of the subarrays the CPU sample covers
     run.sub = []
     for b in picks:
         ufb = Uc[off[b]:off[b + 1]].copy()
-        run.sub.append((int(b), ufb, r_host[off[b]:off[b + 1]].copy(), y32[b]))
+        run.sub.append((int(b), ufb, r_host[off[b]:off[b + 1]].copy(), y32[b],
+                        y64_picked[int(b)]))
     run.f, run.c = f, c
     del U_host, Uc, ufs
     lib.ccfj_batch_graph_cache_clear()
@@ -870,24 +876,25 @@ def cpu_batch(run, ref, threads):
     t = 0.0
     terms = 0
     outs, gpu, y64 = [], [], []
-    for b, ufb, rb, y32b in run.sub:
+    for b, ufb, rb, y32b, y64b in run.sub:
         dt, o = ref_noise_cols(ref, ufb, rb, run.c, run.f, cols, threads)
         t += dt
         terms += len(rb) * len(cols) * len(run.c)
         outs.append(o)
         gpu.append(y32b[:, cols])
+        y64.append(y64b[:, cols])
     run.res["cpu_baseline"] = cpu_line(
         terms, t, threads, "reference fj_noise on 8 subarrays stratified by size (%s pairs), %d "
         "evenly spaced of %d frequencies each (one per thread)" % (
             ",".join(str(len(x[2])) for x in run.sub), len(cols), nf))
     run.ref_out = np.concatenate(outs, axis=1)
     run.gpu_cols = np.concatenate(gpu, axis=1)
-    run.y64_cols = None
+    run.y64_cols = np.concatenate(y64, axis=1)
     run.res["accuracy"]["fjcpu_sample"] = "8 subarrays x %d frequencies" % len(cols)
     jobs = []
     mid = len(cols) // 2
     for k in range(0, len(run.sub), 2):
-        b, ufb, rb, _ = run.sub[k]
+        b, ufb, rb = run.sub[k][:3]
         jobs.append((("noise", dict(uf=ufb[:, cols[[mid]]], r=rb, c=run.c, f=run.f[cols[[mid]]])),
                      (slice(None), [k * len(cols) + mid])))
     run.oracle_jobs = jobs
@@ -904,9 +911,12 @@ def finish_batch(run, oracle_outs):
         er.append(_err(run.ref_out[sl], o))
     acc["err_vs_oracle"] = float(max(eg))
     acc["fjcpu_err_vs_oracle"] = float(max(er))
+    # FJcpu's own error on the columns it was compared on (against the FP64
+    # form, which the oracle pins), and on the oracle's columns
+    acc["fjcpu_err_vs_fp64"] = _err(run.ref_out, run.y64_cols)
+    own = max(acc["fjcpu_err_vs_oracle"], acc["fjcpu_err_vs_fp64"])
     acc["fjcpu_check"] = ("err_vs_fjcpu %.2e <= FJcpu's own error %.2e + 1e-4: %s" %
-                          (acc["err_vs_fjcpu"], acc["fjcpu_err_vs_oracle"],
-                           acc["err_vs_fjcpu"] <= acc["fjcpu_err_vs_oracle"] + 1e-4))
+                          (acc["err_vs_fjcpu"], own, acc["err_vs_fjcpu"] <= own + 1e-4))
     return run.res
 
 
