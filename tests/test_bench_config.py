@@ -107,3 +107,33 @@ def test_oracle_column_helpers_equal_full_oracle():
     sub = O.mwfj_window_columns(m["u"], m["r"], m["c"], m["f"], m["Fs"], m["winl"][1],
                                 m["winr"][1], [2, 5, 9], m["taper"])
     assert np.array_equal(sub, full[1][:, [2, 5, 9]], equal_nan=True)
+
+
+def test_batch_fjcpu_check_uses_the_compared_columns():
+    """Configuration 5's check of FJcpu.cpp: our columns are compared with
+    FJcpu's on the CPU sample's columns, so FJcpu's own error is taken on the
+    same columns (against the FP64 form) as well as on the oracle's."""
+    bench = _bench()
+    rng = np.random.default_rng(0)
+    # normalised columns, as the transforms return them (largest |value| 1)
+    y64 = rng.uniform(-0.5, 0.5, (5, 6))
+    y64[0] = 1.0
+    ours = y64 + 1e-7
+    fjcpu = y64.copy()
+    fjcpu[1] += 0.3  # FJcpu off by 0.3 of the column's largest value
+
+    class Run:
+        pass
+
+    run = Run()
+    run.res = {"accuracy": {}}
+    run.gpu_cols, run.ref_out, run.y64_cols = ours, fjcpu, y64
+    # one oracle column on which FJcpu happens to be accurate
+    run.oracle_jobs = [(None, (slice(None), [2]))]
+    oracle = [y64[:, [2]]]
+    run.ref_out = run.ref_out.copy()
+    run.ref_out[:, 2] = y64[:, 2]
+    acc = bench.finish_batch(run, oracle)["accuracy"]
+    assert acc["fjcpu_err_vs_oracle"] < 1e-12
+    assert abs(acc["fjcpu_err_vs_fp64"] - 0.3) < 1e-9
+    assert acc["fjcpu_check"].endswith("True")
