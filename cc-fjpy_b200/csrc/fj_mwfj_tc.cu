@@ -498,6 +498,8 @@ __global__ void __launch_bounds__(256) mw_tc_prep_kernel(const float2* __restric
   const int half = tc::kSlices * N * 32;  // bytes of the hi (or lo) part
   const int nw2 = N / 2;                  // window slots (rows 2w, 2w+1)
   const int items = kPrepF * nw2 * tc::kChunkI;
+  // unrolled: several items' spectrum loads in flight per thread
+#pragma unroll 4
   for (int t = threadIdx.x; t < items; t += blockDim.x) {
     const int f = t % kPrepF;
     const int w = (t / kPrepF) % nw2;
