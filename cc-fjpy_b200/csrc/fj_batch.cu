@@ -22,6 +22,7 @@
 #include <string>
 #include <vector>
 
+#include "batch_plan.h"
 #include "fj_cells.cuh"
 
 namespace ccfj {
@@ -526,45 +527,10 @@ int batch_run_device(const ccfj_batch_args& a, long long total, cudaStream_t s) 
 }
 
 // ------------------------------------------------- host-memory batches
-// A large batch from host memory is run in groups of consecutive sets, the
-// copy of group g + 1 on a stream of its own while group g computes, so
-// that only the first group's copy is exposed. Group g ends at the first set
-// boundary at or past kGroupEnd[g] of the pairs (the first group is small:
-// its copy is the part that cannot overlap).
-constexpr double kGroupEnd[] = {1.0 / 16, 0.25, 0.5, 0.75, 1.0};
-constexpr size_t kPipelineBytes = (size_t)256 << 20;  // inputs below this: one copy, one pass
-
-struct SetGroup {
-  int b0, b1;                // sets [b0, b1)
-  long long row_lo, row_hi;  // rows of u its pairs read, [row_lo, row_hi]
-};
-
-// Groups of a host batch with one input, or none (one pass) where the
-// input is small, there is one set, or the groups' rows are not disjoint
-// and increasing (a permutation that mixes sets).
+// Large host batches run in groups of sets (batch_plan.h).
 std::vector<SetGroup> plan_groups(const ccfj_batch_args& a, long long total, int nin,
                                   size_t ubytes) {
-  std::vector<SetGroup> g;
-  if (nin != 1 || a.nsets < 2 || ubytes < kPipelineBytes) return g;
-  const long long* off = a.offsets;
-  int b = 0;
-  for (double end : kGroupEnd) {
-    const long long target = (long long)(end * (double)total);
-    const int b0 = b;
-    while (b < a.nsets && (off[b + 1] <= target || b == b0)) ++b;
-    if (end == 1.0) b = a.nsets;
-    if (b <= b0) continue;
-    long long lo = LLONG_MAX, hi = -1;
-    for (long long i = off[b0]; i < off[b]; ++i) {
-      const long long row = a.perm ? a.perm[i] : i;
-      lo = std::min(lo, row);
-      hi = std::max(hi, row);
-    }
-    if (!g.empty() && lo <= g.back().row_hi) return {};
-    g.push_back({b0, b, lo, hi});
-    if (b == a.nsets) break;
-  }
-  return g.size() > 1 ? g : std::vector<SetGroup>{};
+  return plan_set_groups(a.offsets, a.nsets, a.perm, total, nin, ubytes);
 }
 
 // The copy stream of a pipelined batch and its events; waits for every copy
