@@ -814,7 +814,7 @@ def measure_batch(lib, torch, dev, sp, peak, args):
     errs = []
     nan_ok = True
     # the subarrays the CPU sample covers (stratified by size); their FP64
-    # form is kept to judge FJcpu.cpp on the same columns
+    # form is kept to compare FJcpu.cpp with on the same columns
     picks = np.argsort(counts)[np.linspace(0, nsets - 1, 8).round().astype(int)]
     y64_picked = {}
     t0 = time.perf_counter()
