@@ -272,3 +272,15 @@ def test_batch_sets_read_their_own_sorted_pairs(monkeypatch, dtype):
     for (vals, rsorted), uf, r in zip(rec.sets, ufs, rs):
         assert np.array_equal(vals, _expected(uf, r, nf, fstride))
         assert np.array_equal(rsorted, np.sort(r).astype(np.float32))
+
+
+def test_earthquake_result_type_is_float32_or_float64():
+    """MWFJ's float64 result comes from the library's copy-out; any other
+    result type is refused before the call."""
+    from ccfj import _eq
+    rng = np.random.default_rng(0)
+    u = rng.standard_normal((3, 64)).astype(np.float32)
+    r = np.array([1e3, 2e3, 3e3])
+    with pytest.raises(ValueError, match="float32 or float64"):
+        _eq._run(u, r, np.array([2000.0, 3000.0]), np.array([0.1, 0.2]), 1, 1, 0,
+                 dtype=np.int32)
